@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Headline benchmark: symmetric-heap all-reduce GB/s on one B200.
+
+Workload (the plain-method GPU configuration): 64 emulated PEs, 2^20
+elements per PE, in a 4 GiB symmetric heap (64 slices x 64 MiB):
+  float32 SUM  (values N(0,1)),
+  float64 MAX  (values uniform in [-1e6, 1e6]),
+  int64   XOR  (uniform random bits),
+each in the recursive-doubling and the Rabenseifner combine order.
+One step = these 6 reductions.  Algorithmic bytes per reduction are
+2*P*N*sizeof(T) (every source read once, every dest written once), so a
+step moves 5 GiB.  Every launch reads >= 256 MiB, more than the 126 MB
+L2, so no flush is needed between iterations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU implementation of the same
+reductions (its src/shcoll/src code, compiled unmodified into
+oracle/_ref and run over emulated PEs on the host cores) on a bounded
+sample of the workload.  Under torchrun, every rank runs its own
+independent 64-PE team on its own GPU (weak scaling, no data-path
+collective); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "osss-ucx_b200"), os.path.join(ROOT, "oracle"),
+          os.path.join(ROOT, "tests")):
+    sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "reduce/alltoall GB/s vs HBM peak; batched ops/s + p99 latency vs per-call"
+P = 64
+N = 1 << 20
+HEAP = 64 << 20
+OPS = [("sum", "float32", np.float32), ("max", "float64", np.float64), ("xor", "int64", np.int64)]
+ALGOS = ["rec_dbl", "rabenseifner"]
+FALLBACK_HBM = 6650.0
+
+
+def workload_desc(n_gpus):
+    return {"workload": "allreduce over 64 emulated PEs x 2^20 elems/PE: f32 sum N(0,1), "
+                        "f64 max U(-1e6,1e6), i64 xor U(bits); rec_dbl and rabenseifner orders",
+            "npes": P, "nelems_per_pe": N, "heap_bytes": P * HEAP,
+            "ops": [f"{d}:{o}" for o, d, _ in OPS], "algos": ALGOS,
+            "l2": "inputs larger than L2 (>= 256 MiB read per launch), no flush",
+            "parallelism": f"{n_gpus} independent 64-PE teams, one per GPU"}
+
+
+def inputs(seed_base=0):
+    import gen
+    return [gen.normal(np.float32, P, N, 21 + seed_base),
+            gen.uniform(np.float64, P, N, 22 + seed_base, -1e6, 1e6),
+            gen.uniform_int(np.int64, P, N, 23 + seed_base)]
+
+
+def alg_bytes(npes, n, dt):
+    return 2 * npes * n * np.dtype(dt).itemsize
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own shcoll code over emulated PEs
+# ---------------------------------------------------------------------------
+_CPU_INPUTS = {}
+
+
+def cpu_reference_times(n_sample=N, warmup=1, iters=3):
+    """Per-iteration seconds of one step (the 3 ops x 2 orders) of the
+    reference's own shcoll code on P=64 emulated PEs (one pinned pthread
+    each) with n_sample elements per PE.  Returns (step_seconds[iters],
+    bytes_per_step, description, kind)."""
+    import oracle
+    if n_sample not in _CPU_INPUTS:
+        _CPU_INPUTS[n_sample] = inputs_small(n_sample)
+    xs = _CPU_INPUTS[n_sample]
+    tnames = {"float32": "float", "float64": "double", "int64": "int64"}
+    step = np.zeros(iters)
+    nbytes = 0
+    if oracle.Reference.available:
+        R, kind = oracle.Reference(), "reference"
+        for (op, dt, npdt), x in zip(OPS, xs):
+            for algo in ALGOS:
+                _, times = R.reduce(algo, op, x, tname=tnames[dt], warmup=warmup, iters=iters,
+                                    pin=True)
+                step += times
+                nbytes += alg_bytes(P, n_sample, npdt)
+        desc = (f"full workload: 64 emulated PEs (pinned pthreads) x {n_sample} elems/PE, "
+                f"3 ops x 2 orders per step; the reference's src/shcoll/src code compiled "
+                f"unmodified (oracle/_ref); {iters} timed steps after {warmup} warm-up")
+    else:
+        rs, kind = oracle.Restatement(), "port"
+        for (op, dt, npdt), x in zip(OPS, xs):
+            for algo in ALGOS:
+                for _ in range(warmup):
+                    rs.reduce(algo, op, x)
+                for k in range(iters):
+                    t0 = time.perf_counter()
+                    rs.reduce(algo, op, x)
+                    step[k] += time.perf_counter() - t0
+                nbytes += alg_bytes(P, n_sample, npdt)
+        desc = f"C restatement (oracle/shcoll_oracle.c), single thread, 64 PEs x {n_sample} elems/PE"
+    return step, nbytes, desc, kind
+
+
+def inputs_small(n):
+    import gen
+    return [gen.normal(np.float32, P, n, 21), gen.uniform(np.float64, P, n, 22, -1e6, 1e6),
+            gen.uniform_int(np.int64, P, n, 23)]
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    step, nbytes, desc, kind = cpu_reference_times(warmup=args.warmup, iters=args.steps)
+    value = nbytes / float(np.median(step)) / 1e9
+    cores = os.cpu_count() or 1 if kind == "reference" else 1
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(float(np.median(step)) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64+i64", "data": "synthetic (seeded per PE)",
+            "config": workload_desc(args.gpus),
+            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": kind,
+                             "sample": desc},
+            "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    B.init(P, HEAP)
+    team = (0, 1, P)
+    xs = inputs(seed_base=rank * 100)
+    src, dst = B.malloc(8 * N), B.malloc(8 * N)
+    srcs = []
+    for x in xs:
+        off = B.malloc(x[0].nbytes)
+        B.put_rows(off, x, team=team)
+        srcs.append(off)
+    stream_ptr = B.stream()
+    s = torch.cuda.ExternalStream(stream_ptr)
+    calls = [(op, dt, algo, srcs[i], npdt) for i, (op, dt, npdt) in enumerate(OPS) for algo in ALGOS]
+    step_bytes = sum(alg_bytes(P, N, c[4]) for c in calls)
+
+    def step(evs=None):
+        for j, (op, dt, algo, so, _) in enumerate(calls):
+            if evs is not None:
+                evs[j][0].record(s)
+            B.reduce(op, dt, algo, dst, so, N, team=team, stream=stream_ptr)
+            if evs is not None:
+                evs[j][1].record(s)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    B.quiet()
+    barrier()
+
+    per_call = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                 for _ in calls] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = B.launch_count()
+    start.record(s)
+    for k in range(args.steps):
+        step(per_call[k])
+    end.record(s)
+    B.quiet()
+    launches = B.launch_count() - launches0
+    clk = clocks.stop()
+    barrier()
+    ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = step_bytes * args.steps * world / (ms / 1e3) / 1e9
+
+    # per-kernel durations (the reduce kernel of each (dtype, op, order))
+    durs = {}
+    for j, (op, dt, algo, _, npdt) in enumerate(calls):
+        d = [per_call[k][j][0].elapsed_time(per_call[k][j][1]) for k in range(args.steps)]
+        durs[f"{dt}:{op}:{algo}"] = (float(np.mean(d)), alg_bytes(P, N, npdt))
+    dom = max(durs, key=lambda k: durs[k][0])
+    dom_ms, dom_bytes = durs[dom]
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "reduce_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dom)
+
+    # e2e: host buffers in, reduce, host buffers out, through the C ABI
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned_in = [torch.from_numpy(x).pin_memory() for x in xs]
+        pinned_out = [torch.empty(x.shape, dtype=torch.from_numpy(x[:1]).dtype).pin_memory() for x in xs]
+        h2d = d2h = 0
+
+        def e2e_step():
+            nonlocal h2d, d2h
+            h2d = d2h = 0
+            for i, (op, dt, npdt) in enumerate(OPS):
+                for algo in ALGOS:
+                    nb = xs[i][0].nbytes
+                    B.lib.b200shm_put_host(0, 1, P, srcs[i], pinned_in[i].data_ptr(), nb, stream_ptr)
+                    B.reduce(op, dt, algo, dst, srcs[i], N, team=team, stream=stream_ptr)
+                    B.lib.b200shm_get_host(pinned_out[i].data_ptr(), 0, 1, P, dst, nb, stream_ptr)
+                    h2d += P * nb
+                    d2h += P * nb
+        e2e_step()
+        B.quiet()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e1.record(s)
+        B.quiet()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": round(step_bytes * args.e2e_steps * world / (ems / 1e3) / 1e9, 3),
+               "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "steps": args.e2e_steps, "ms_per_step": round(ems / args.e2e_steps, 3),
+               "path": "b200shm_put_host -> b200shm_reduce -> b200shm_get_host, pinned host rows"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        step_s, nbytes, desc, kind = cpu_reference_times()
+        cpu = {"value": round(nbytes / float(np.median(step_s)) / 1e9, 4), "unit": "GB/s",
+               "cores": (os.cpu_count() or 1) if kind == "reference" else 1, "kind": kind,
+               "sample": desc, "seconds_per_step": round(float(np.median(step_s)), 4)}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64+i64", "data": "synthetic (seeded per PE: N(0,1), U(+-1e6), U(bits))",
+            "config": workload_desc(world),
+            "roofline": {"bound": "hbm", "kernel": f"k_reduce {dom}", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4)},
+            "per_kernel_ms": {k: round(v[0], 4) for k, v in durs.items()},
+            "per_kernel_gbs": {k: round(v[1] / (v[0] / 1e3) / 1e9, 1) for k, v in durs.items()},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+/*
+ * b200shm.h -- C ABI of the B200 OpenSHMEM collective and atomic engine.
+ *
+ * Model.  `npes` PEs are emulated on one GPU.  Each PE's symmetric heap is
+ * the slice [pe * slice, (pe + 1) * slice) of one HBM arena, so a symmetric
+ * object is one offset `off` that is valid in every slice.  A team (or an
+ * active set) is the member list pe_start + i * pe_stride, i < pe_size.
+ * A collective is issued ONCE for the whole team, not once per PE: the
+ * per-PE OpenSHMEM calls (include/shmem.h, include/shcoll_b200.h) aggregate
+ * the members' calls into one of these entry points.
+ *
+ * Streams.  `stream` is a cudaStream_t passed as void*.  NULL means the
+ * library's own stream and a blocking call (the call returns when the
+ * result is in every member's dest, as the OpenSHMEM routines do).  A
+ * non-NULL stream makes the call stream-ordered and asynchronous.
+ *
+ * Errors.  Every int-returning entry point returns B200SHM_OK (0) or a
+ * negative enum b200shm_status; b200shm_last_error() describes the last
+ * failure of the calling thread.
+ *
+ * Each declaration cites the reference (BTMichalowicz/osss-ucx) interface
+ * it replaces.
+ */
+#ifndef B200SHM_H
+#define B200SHM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../osss-ucx_b200/csrc/b200shm_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* lifecycle and heap                                                      */
+/* ---------------------------------------------------------------------- */
+
+#define B200SHM_INIT_MANAGED 0x1 /* arena in CUDA managed memory (host-visible) */
+
+/* Create the arena of npes slices of heap_bytes_per_pe (rounded up to
+ * 2 MiB) on the current CUDA device.  Replaces shmemc_heaps_init
+ * (src/shmemc/heaps.c:33-52) and register_symmetric_heap
+ * (src/shmemc/ucx/init.c:174-218); the heap size plays the role of
+ * SHMEM_SYMMETRIC_SIZE (src/shmemc/env.c:117-119). */
+int b200shm_init(int npes, uint64_t heap_bytes_per_pe, int flags);
+/* Release everything (src/shmemc/init.c shmemc_finalize). */
+int b200shm_finalize(void);
+int b200shm_initialized(void);
+int b200shm_n_pes(void);                 /* shmem_n_pes, src/api/info.c */
+uint64_t b200shm_heap_slice(void);       /* bytes per PE slice */
+void *b200shm_heap_base(void);           /* device address of slice 0 */
+/* Device address of offset `off` in PE `pe`'s slice; NULL if out of range.
+ * Plays the role of shmem_ptr (src/api/ptr.c) and of the region lookup
+ * translate_region_address (src/shmemc/ucx/comms.c:99-112). */
+void *b200shm_ptr(int pe, uint64_t off);
+const char *b200shm_last_error(void);
+/* Wait for all work on the library stream (shmem_quiet semantics for the
+ * device, src/shmemc/ucx/comms.c:205-227). */
+int b200shm_quiet(void);
+/* Number of kernels this library has launched since it was loaded. */
+unsigned long long b200shm_launch_count(void);
+/* The library stream, as a cudaStream_t. */
+void *b200shm_stream(void);
+
+/* Symmetric allocation: the same offset in every slice.  Replaces
+ * shmem_malloc / shmem_align / shmem_free (src/api/shmalloc.c:47-195) and
+ * the dlmalloc mspace behind them (src/api/allocator/memalloc.c:29-93). */
+int b200shm_malloc(uint64_t bytes, uint64_t align, uint64_t *off);
+int b200shm_free(uint64_t off);
+uint64_t b200shm_heap_free_bytes(void);
+
+/* Host <-> symmetric heap copies for pe_count PEs pe_start + i*pe_stride:
+ * host row i (bytes_per_pe bytes) <-> offset `off` of member i.  These are
+ * how host buffers enter and leave the arena (the put/get of
+ * src/shmemc/ucx/comms.c:677-737 with a host-side peer). */
+int b200shm_put_host(int pe_start, int pe_stride, int pe_count, uint64_t off,
+                     const void *host_src, uint64_t bytes_per_pe, void *stream);
+int b200shm_get_host(void *host_dst, int pe_start, int pe_stride, int pe_count,
+                     uint64_t off, uint64_t bytes_per_pe, void *stream);
+/* Fill bytes_per_pe bytes at `off` of pe_count members with `byte`. */
+int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off,
+                   int byte, uint64_t bytes_per_pe, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* collectives (one call per team)                                         */
+/* ---------------------------------------------------------------------- */
+
+/* All-reduce of nelems elements: every member's dest gets the reduction of
+ * all members' sources, computed in the combine order of `algo`.
+ * Replaces reduce_helper_<T>_<op>_{linear,binomial,rec_dbl,rabenseifner,
+ * rabenseifner2} (src/shcoll/src/reduce.c:55-724) behind
+ * shcoll_<T>_<op>_reduce_<algo> (reduce.c:1078-1102) and
+ * shcoll_<T>_<op>_to_all_<algo> (reduce.c:931-955).  dest_off == src_off
+ * (in place) is allowed; other overlaps are rejected. */
+int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_stride,
+                   int pe_size, uint64_t dest_off, uint64_t src_off,
+                   uint64_t nelems, void *stream);
+
+/* Fixed-size allgather: member j's dest[k*nbytes ..] = member k's source.
+ * Replaces fcollect_helper_* (src/shcoll/src/fcollect.c:32-484) behind
+ * shcoll_fcollect{32,64}_<algo>, shcoll_<T>_fcollect_<algo> and
+ * shcoll_fcollectmem_<algo> (fcollect.c:492-653). */
+int b200shm_fcollect(int pe_start, int pe_stride, int pe_size,
+                     uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
+                     void *stream);
+
+/* All-to-all of nbytes blocks: member j's dest block k = member k's source
+ * block j.  Replaces alltoall_helper_* (src/shcoll/src/alltoall.c:75-201)
+ * behind shcoll_alltoall{32,64}_<algo>, shcoll_<T>_alltoall_<algo> and
+ * shcoll_alltoallmem_<algo> (alltoall.c:242-387). */
+int b200shm_alltoall(int pe_start, int pe_stride, int pe_size,
+                     uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
+                     void *stream);
+
+/* Strided all-to-all: element t from member k to member l moves
+ * src_k[(l*nelems + t)*sst] -> dest_l[(k*nelems + t)*dst] (elements of
+ * elem_size bytes); other dest elements are untouched.  Replaces
+ * alltoalls_helper_* (src/shcoll/src/alltoalls.c:54-297, index rule 39-50)
+ * behind shcoll_alltoalls{32,64}_<algo> and shcoll_<T>_alltoalls_<algo>
+ * (alltoalls.c:303-435). */
+int b200shm_alltoalls(int pe_start, int pe_stride, int pe_size,
+                      uint64_t dest_off, uint64_t src_off, int64_t dst,
+                      int64_t sst, uint64_t nelems, uint64_t elem_size,
+                      void *stream);
+
+/* Broadcast nbytes from member `root`'s source to every other member's
+ * dest (the root's dest is left untouched).  Replaces broadcast_helper_*
+ * (src/shcoll/src/broadcast.c:58-599). */
+int b200shm_broadcast(int root, int pe_start, int pe_stride, int pe_size,
+                      uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
+                      void *stream);
+
+/* Barrier among the members, run on the device by one PE context per
+ * member over flag words with the given algorithm's message pattern, with
+ * a bounded spin.  Replaces barrier_sync_helper_* (src/shcoll/src/
+ * barrier.c:56-266) behind shcoll_barrier[_all]_<algo>, shcoll_sync[_all]
+ * and shcoll_team_sync_<algo> (barrier.c:279-366).  Returns
+ * B200SHM_ERR_TIMEOUT if a member's wait ran out of budget. */
+int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size,
+                    void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* atomics                                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* A batch of nops atomic operations on symmetric objects of `dtype`
+ * (4- or 8-byte integers; F32/F64 for SWAP/SET/FETCH): operation k acts on
+ * the element at offset off[k] (bytes) of PE pe[k].  value/cond/fetched are
+ * arrays of nops elements (cond only for CSWAP; fetched may be NULL for the
+ * non-fetching forms).  All arrays are DEVICE pointers.  Replaces one
+ * shmem_<T>_atomic_<op> per element (the src/api/atomics files ->
+ * shmemc_ctx_{fadd,add,swap,cswap,fetch,set,and,or,xor}, src/shmemc/ucx/
+ * comms.c:409-671), each of which is a blocking round trip there. */
+int b200shm_amo_batch(int amo, int dtype, uint64_t nops, const int32_t *pe,
+                      const uint64_t *off, const void *value, const void *cond,
+                      void *fetched, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,197 @@
+"""Python binding of the C ABI in include/b200shm.h (ctypes).
+
+This is how the tests and the benchmark drive the engine: every call goes
+through libb200shm.so.  There is no fallback of any kind -- if the library
+cannot be loaded, importing this module raises.
+
+Usage:
+    import b200shm as B
+    B.init(npes=64, heap_bytes=64 << 20)
+    src = B.malloc(N * 4); dst = B.malloc(N * 4)
+    B.put_rows(src, x)                      # x: [npes, N] numpy array
+    B.reduce("sum", "float32", "rec_dbl", dst, src, N, team=(0, 1, 64))
+    y = B.get_rows(dst, N * 4, np.float32, team=(0, 1, 64))
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libb200shm.so")
+
+DTYPES = ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64",
+          "float32", "float64", "float80", "complex64", "complex128"]
+OPS = ["and", "or", "xor", "min", "max", "sum", "prod"]
+ALGOS = ["linear", "binomial", "rec_dbl", "rabenseifner", "rabenseifner2"]
+BARRIER_ALGOS = ["linear", "complete_tree", "binomial_tree", "knomial_tree", "dissemination"]
+AMOS = ["fetch_add", "add", "fetch_inc", "inc", "swap", "cswap", "set", "fetch", "fetch_and",
+        "and", "fetch_or", "or", "fetch_xor", "xor"]
+STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_UNSUPPORTED", -3: "ERR_NOMEM", -4: "ERR_CUDA",
+          -5: "ERR_STATE", -6: "ERR_TIMEOUT", -7: "ERR_BUSY"}
+
+
+class B200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(LIB_PATH + " is missing: build it with `python osss-ucx_b200/build.py`")
+    L = ctypes.CDLL(LIB_PATH)
+    ci, u64, i64, vp = ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, ctypes.c_void_p
+    sig = {
+        "b200shm_init": (ci, [ci, u64, ci]),
+        "b200shm_finalize": (ci, []),
+        "b200shm_initialized": (ci, []),
+        "b200shm_n_pes": (ci, []),
+        "b200shm_heap_slice": (u64, []),
+        "b200shm_heap_base": (vp, []),
+        "b200shm_ptr": (vp, [ci, u64]),
+        "b200shm_last_error": (ctypes.c_char_p, []),
+        "b200shm_quiet": (ci, []),
+        "b200shm_launch_count": (ctypes.c_ulonglong, []),
+        "b200shm_stream": (vp, []),
+        "b200shm_malloc": (ci, [u64, u64, ctypes.POINTER(u64)]),
+        "b200shm_free": (ci, [u64]),
+        "b200shm_heap_free_bytes": (u64, []),
+        "b200shm_put_host": (ci, [ci, ci, ci, u64, vp, u64, vp]),
+        "b200shm_get_host": (ci, [vp, ci, ci, ci, u64, u64, vp]),
+        "b200shm_memset": (ci, [ci, ci, ci, u64, ci, u64, vp]),
+        "b200shm_reduce": (ci, [ci, ci, ci, ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_fcollect": (ci, [ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_alltoall": (ci, [ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_alltoalls": (ci, [ci, ci, ci, u64, u64, i64, i64, u64, u64, vp]),
+        "b200shm_broadcast": (ci, [ci, ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_barrier": (ci, [ci, ci, ci, ci, vp]),
+        "b200shm_amo_batch": (ci, [ci, ci, u64, vp, vp, vp, vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def _check(rc):
+    if rc != 0:
+        raise B200Error(rc, lib.b200shm_last_error().decode())
+    return rc
+
+
+def _team(team):
+    if team is None:
+        return 0, 1, lib.b200shm_n_pes()
+    return team
+
+
+def init(npes, heap_bytes, managed=False):
+    return _check(lib.b200shm_init(npes, heap_bytes, 1 if managed else 0))
+
+
+def finalize():
+    return _check(lib.b200shm_finalize())
+
+
+def initialized():
+    return bool(lib.b200shm_initialized())
+
+
+def n_pes():
+    return lib.b200shm_n_pes()
+
+
+def malloc(nbytes, align=256):
+    off = ctypes.c_uint64(0)
+    _check(lib.b200shm_malloc(nbytes, align, ctypes.byref(off)))
+    return off.value
+
+
+def free(off):
+    return _check(lib.b200shm_free(off))
+
+
+def launch_count():
+    """Kernels launched by libb200shm.so since it was loaded."""
+    return lib.b200shm_launch_count()
+
+
+def stream():
+    """The library stream (a cudaStream_t as an int)."""
+    return lib.b200shm_stream()
+
+
+def quiet():
+    return _check(lib.b200shm_quiet())
+
+
+def ptr(pe, off):
+    return lib.b200shm_ptr(pe, off)
+
+
+def put_rows(off, x, team=None, stream=None):
+    """Copy host rows x[i] into member i's slice at `off`."""
+    start, stride, size = _team(team)
+    x = np.ascontiguousarray(x)
+    assert x.shape[0] == size
+    return _check(lib.b200shm_put_host(start, stride, size, off, x.ctypes.data,
+                                       x[0].nbytes if size else 0, stream))
+
+
+def get_rows(off, row_bytes, dtype, team=None, stream=None, out=None):
+    """Copy row_bytes at `off` of every member into a host [size, ...] array."""
+    start, stride, size = _team(team)
+    dt = np.dtype(dtype)
+    if out is None:
+        out = np.empty((size, row_bytes // dt.itemsize), dtype=dt)
+    _check(lib.b200shm_get_host(out.ctypes.data, start, stride, size, off, row_bytes, stream))
+    return out
+
+
+def memset(off, byte, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_memset(start, stride, size, off, byte, nbytes, stream))
+
+
+def reduce(op, dtype, algo, dest, src, nelems, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_reduce(OPS.index(op), DTYPES.index(dtype), ALGOS.index(algo),
+                                     start, stride, size, dest, src, nelems, stream))
+
+
+def fcollect(dest, src, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_fcollect(start, stride, size, dest, src, nbytes, stream))
+
+
+def alltoall(dest, src, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_alltoall(start, stride, size, dest, src, nbytes, stream))
+
+
+def alltoalls(dest, src, dst, sst, nelems, elem_size, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_alltoalls(start, stride, size, dest, src, dst, sst, nelems,
+                                        elem_size, stream))
+
+
+def broadcast(root, dest, src, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_broadcast(root, start, stride, size, dest, src, nbytes, stream))
+
+
+def barrier(algo="binomial_tree", team=None, stream=None):
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_barrier(BARRIER_ALGOS.index(algo), start, stride, size, stream))
+
+
+def amo_batch(amo, dtype, nops, pe_dev, off_dev, value_dev=None, cond_dev=None,
+              fetched_dev=None, stream=None):
+    """Device-array AMO batch; *_dev are device addresses (ints)."""
+    return _check(lib.b200shm_amo_batch(AMOS.index(amo), DTYPES.index(dtype), nops, pe_dev,
+                                        off_dev, value_dev, cond_dev, fetched_dev, stream))

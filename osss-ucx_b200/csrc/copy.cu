@@ -1,0 +1,295 @@
+/*
+ * copy.cu -- the data-movement collectives: fcollect, alltoall, strided
+ * alltoall and broadcast.
+ *
+ * In the reference every byte crosses a process boundary as a UCX put
+ * (fcollect: log2(P) Bruck rounds plus an in-place byte rotation,
+ * src/shcoll/src/fcollect.c:370-403 and util/rotate.c:22-54; alltoall:
+ * P-1 puts per PE, alltoall.c:75-110; strided alltoall: one put per
+ * element, alltoalls.c:54-90).  The result of each is a fixed permutation
+ * of bytes that does not depend on the algorithm, so here each collective
+ * is one copy kernel that moves every byte once from its source slice to
+ * its final place: no rounds, no intermediate copies, no rotation.
+ *
+ * Copies run in 16-byte vectors when every base offset and size is a
+ * multiple of 16, else in bytes (or elements for the strided form).
+ */
+#include <stdint.h>
+
+#include "internal.cuh"
+
+namespace b200 {
+namespace {
+
+__device__ __forceinline__ uint4 ld16(const char *p) {
+  uint4 u;
+  asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(u.x), "=r"(u.y), "=r"(u.z), "=r"(u.w)
+      : "l"(p));
+  return u;
+}
+__device__ __forceinline__ void st16(char *p, uint4 u) {
+  asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y), "r"(u.z),
+               "r"(u.w)
+               : "memory");
+}
+
+/* fcollect: member j's dest[k*nbytes + b] = member k's src[b].
+ * blockIdx.y = source member k; each thread reads one vector of k's
+ * source once and writes it into every member's dest. */
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_fcollect(const char *src0, char *dst0, uint64_t step,
+                                                  int P, uint64_t nbytes) {
+  const int k = blockIdx.y;
+  const char *src = src0 + (uint64_t)k * step;
+  char *dst = dst0 + (uint64_t)k * nbytes;
+  const uint64_t n = VEC ? nbytes / 16 : nbytes;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    if constexpr (VEC) {
+      const uint4 u = ld16(src + v * 16);
+      for (int j = 0; j < P; j++) st16(dst + (uint64_t)j * step + v * 16, u);
+    } else {
+      const char c = src[v];
+      for (int j = 0; j < P; j++) dst[(uint64_t)j * step + v] = c;
+    }
+  }
+}
+
+/* alltoall: member j's dest[k*B + b] = member k's src[j*B + b].
+ * blockIdx.y = pair index k*P + j; blockIdx.x strides over the block. */
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_alltoall(const char *src0, char *dst0, uint64_t step,
+                                                  int P, uint64_t B) {
+  const int k = blockIdx.y / P, j = blockIdx.y % P;
+  const char *src = src0 + (uint64_t)k * step + (uint64_t)j * B;
+  char *dst = dst0 + (uint64_t)j * step + (uint64_t)k * B;
+  const uint64_t n = VEC ? B / 16 : B;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (VEC) {
+    /* four vectors in flight per thread */
+    for (; v + 3 * stride < n; v += 4 * stride) {
+      uint4 u0 = ld16(src + v * 16), u1 = ld16(src + (v + stride) * 16);
+      uint4 u2 = ld16(src + (v + 2 * stride) * 16), u3 = ld16(src + (v + 3 * stride) * 16);
+      st16(dst + v * 16, u0);
+      st16(dst + (v + stride) * 16, u1);
+      st16(dst + (v + 2 * stride) * 16, u2);
+      st16(dst + (v + 3 * stride) * 16, u3);
+    }
+    for (; v < n; v += stride) st16(dst + v * 16, ld16(src + v * 16));
+  } else {
+    for (; v < n; v += stride) dst[v] = src[v];
+  }
+}
+
+/* strided alltoall (alltoalls.c:39-50, 78-83): element t from member k to
+ * member l: src_k[(l*n + t)*sst] -> dest_l[(k*n + t)*dst].
+ * blockIdx.y = pair index k*P + l. */
+template <class E>
+__global__ void __launch_bounds__(256) k_alltoalls(const char *src0, char *dst0, uint64_t step,
+                                                   int P, uint64_t n, int64_t dst, int64_t sst) {
+  const int k = blockIdx.y / P, l = blockIdx.y % P;
+  const E *src = (const E *)(src0 + (uint64_t)k * step) + (uint64_t)l * n * (uint64_t)sst;
+  E *d = (E *)(dst0 + (uint64_t)l * step) + (uint64_t)k * n * (uint64_t)dst;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x)
+    d[t * (uint64_t)dst] = src[t * (uint64_t)sst];
+}
+
+/* strided alltoall with an element size that is not 1/2/4/8/16 bytes */
+__global__ void __launch_bounds__(256) k_alltoalls_bytes(const char *src0, char *dst0,
+                                                         uint64_t step, int P, uint64_t n,
+                                                         int64_t dst, int64_t sst, uint64_t es) {
+  const int k = blockIdx.y / P, l = blockIdx.y % P;
+  const char *src = src0 + (uint64_t)k * step + (uint64_t)l * n * (uint64_t)sst * es;
+  char *d = dst0 + (uint64_t)l * step + (uint64_t)k * n * (uint64_t)dst * es;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n * es;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t t = x / es, b = x % es;
+    d[t * (uint64_t)dst * es + b] = src[t * (uint64_t)sst * es + b];
+  }
+}
+
+/* broadcast: every member but the root gets the root's source */
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_broadcast(const char *src, char *dst0, uint64_t step,
+                                                   int P, int root, uint64_t nbytes) {
+  const uint64_t n = VEC ? nbytes / 16 : nbytes;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    if constexpr (VEC) {
+      const uint4 u = ld16(src + v * 16);
+      for (int j = 0; j < P; j++)
+        if (j != root) st16(dst0 + (uint64_t)j * step + v * 16, u);
+    } else {
+      const char c = src[v];
+      for (int j = 0; j < P; j++)
+        if (j != root) dst0[(uint64_t)j * step + v] = c;
+    }
+  }
+}
+
+/* CTAs along x for a per-pair / per-member extent of n work items, so that
+ * the whole grid is about `want` CTAs. */
+unsigned x_blocks(uint64_t n, uint64_t ypairs, uint64_t want) {
+  uint64_t per = (n + 255) / 256;
+  uint64_t cap = want / (ypairs ? ypairs : 1);
+  if (cap < 1) cap = 1;
+  if (per > cap) per = cap;
+  return (unsigned)(per < 1 ? 1 : per);
+}
+
+}  // namespace
+
+int fcollect_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint64_t src_off,
+                    uint64_t nbytes, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, P);
+  if (rc) return rc;
+  if (nbytes > st().slice / (uint64_t)P) return fail(B200SHM_ERR_ARG, "fcollect: too large");
+  if ((rc = check_extent(src_off, nbytes, "fcollect source"))) return rc;
+  if ((rc = check_extent(dest_off, nbytes * (uint64_t)P, "fcollect dest"))) return rc;
+  if (overlaps(dest_off, nbytes * (uint64_t)P, src_off, nbytes))
+    return fail(B200SHM_ERR_ARG, "fcollect: dest and source overlap");
+  if (nbytes == 0) return B200SHM_OK;
+  if (P > 65535) return fail(B200SHM_ERR_UNSUPPORTED, "fcollect: more than 65535 members");
+  Members m = members(pe_start, pe_stride, P);
+  const bool vec = ((src_off | dest_off | nbytes | m.step) & 15u) == 0;
+  const uint64_t n = vec ? nbytes / 16 : nbytes;
+  dim3 grid(x_blocks(n, P, 8ull * st().sm_count * 4), P);
+  if (vec)
+    k_fcollect<true><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, nbytes);
+  else
+    k_fcollect<false><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, nbytes);
+  count_launch();
+  return B200SHM_OK;
+}
+
+int alltoall_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint64_t src_off,
+                    uint64_t B, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, P);
+  if (rc) return rc;
+  if (B > st().slice / (uint64_t)P) return fail(B200SHM_ERR_ARG, "alltoall: too large");
+  if ((rc = check_extent(src_off, B * (uint64_t)P, "alltoall source"))) return rc;
+  if ((rc = check_extent(dest_off, B * (uint64_t)P, "alltoall dest"))) return rc;
+  if (overlaps(dest_off, B * (uint64_t)P, src_off, B * (uint64_t)P))
+    return fail(B200SHM_ERR_ARG, "alltoall: dest and source overlap");
+  if (B == 0) return B200SHM_OK;
+  if ((uint64_t)P * (uint64_t)P > 65535)
+    return fail(B200SHM_ERR_UNSUPPORTED, "alltoall: more than 255 members");
+  Members m = members(pe_start, pe_stride, P);
+  const bool vec = ((src_off | dest_off | B | m.step) & 15u) == 0;
+  const uint64_t n = vec ? B / 16 : B;
+  const uint64_t pairs = (uint64_t)P * P;
+  dim3 grid(x_blocks(vec ? (n + 3) / 4 : n, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
+  if (vec)
+    k_alltoall<true><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, B);
+  else
+    k_alltoall<false><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, B);
+  count_launch();
+  return B200SHM_OK;
+}
+
+int alltoalls_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint64_t src_off,
+                     int64_t dst, int64_t sst, uint64_t n, uint64_t es, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, P);
+  if (rc) return rc;
+  if (dst < 1 || sst < 1 || es < 1)
+    return fail(B200SHM_ERR_ARG, "alltoalls: strides and element size must be positive");
+  const uint64_t lim = st().slice;
+  /* extent touched: (P*n - 1)*stride + 1 elements */
+  if (n > lim / es / (uint64_t)P) return fail(B200SHM_ERR_ARG, "alltoalls: too large");
+  if (n == 0) return B200SHM_OK;
+  const uint64_t cnt = (uint64_t)P * n;
+  if ((uint64_t)dst > lim / cnt || (uint64_t)sst > lim / cnt)
+    return fail(B200SHM_ERR_ARG, "alltoalls: stride too large");
+  const uint64_t dbytes = ((cnt - 1) * (uint64_t)dst + 1) * es;
+  const uint64_t sbytes = ((cnt - 1) * (uint64_t)sst + 1) * es;
+  if ((rc = check_extent(src_off, sbytes, "alltoalls source"))) return rc;
+  if ((rc = check_extent(dest_off, dbytes, "alltoalls dest"))) return rc;
+  if (overlaps(dest_off, dbytes, src_off, sbytes))
+    return fail(B200SHM_ERR_ARG, "alltoalls: dest and source overlap");
+  if ((uint64_t)P * (uint64_t)P > 65535)
+    return fail(B200SHM_ERR_UNSUPPORTED, "alltoalls: more than 255 members");
+  Members m = members(pe_start, pe_stride, P);
+  const uint64_t pairs = (uint64_t)P * P;
+  dim3 grid(x_blocks(n, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
+  const char *sp = m.first + src_off;
+  char *dp = m.first + dest_off;
+  const bool al = ((src_off | dest_off | m.step) % es) == 0;
+  if (al && es == 8)
+    k_alltoalls<uint64_t><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
+  else if (al && es == 4)
+    k_alltoalls<uint32_t><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
+  else if (al && es == 2)
+    k_alltoalls<uint16_t><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
+  else if (es == 1)
+    k_alltoalls<uint8_t><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
+  else if (al && es == 16)
+    k_alltoalls<uint4><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
+  else {
+    dim3 g2(x_blocks(n * es, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
+    k_alltoalls_bytes<<<g2, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst, es);
+  }
+  count_launch();
+  return B200SHM_OK;
+}
+
+int broadcast_launch(int root, int pe_start, int pe_stride, int P, uint64_t dest_off,
+                     uint64_t src_off, uint64_t nbytes, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, P);
+  if (rc) return rc;
+  if (root < 0 || root >= P) return fail(B200SHM_ERR_ARG, "broadcast: root %d not a member", root);
+  if ((rc = check_extent(src_off, nbytes, "broadcast source"))) return rc;
+  if ((rc = check_extent(dest_off, nbytes, "broadcast dest"))) return rc;
+  if (dest_off != src_off && overlaps(dest_off, nbytes, src_off, nbytes))
+    return fail(B200SHM_ERR_ARG, "broadcast: dest and source overlap");
+  if (nbytes == 0 || P == 1) return B200SHM_OK;
+  Members m = members(pe_start, pe_stride, P);
+  const bool vec = ((src_off | dest_off | nbytes | m.step) & 15u) == 0;
+  const uint64_t n = vec ? nbytes / 16 : nbytes;
+  const char *src = m.first + (uint64_t)root * m.step + src_off;
+  if (vec)
+    k_broadcast<true><<<grid_for(n, 256, 8), 256, 0, s>>>(src, m.first + dest_off, m.step, P, root, nbytes);
+  else
+    k_broadcast<false><<<grid_for(n, 256, 8), 256, 0, s>>>(src, m.first + dest_off, m.step, P, root, nbytes);
+  count_launch();
+  return B200SHM_OK;
+}
+
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" {
+
+int b200shm_fcollect(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                     uint64_t src_off, uint64_t nbytes, void *stream) {
+  int rc = fcollect_launch(pe_start, pe_stride, pe_size, dest_off, src_off, nbytes,
+                           pick_stream(stream));
+  return rc ? rc : finish(stream, "b200shm_fcollect");
+}
+
+int b200shm_alltoall(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                     uint64_t src_off, uint64_t nbytes, void *stream) {
+  int rc = alltoall_launch(pe_start, pe_stride, pe_size, dest_off, src_off, nbytes,
+                           pick_stream(stream));
+  return rc ? rc : finish(stream, "b200shm_alltoall");
+}
+
+int b200shm_alltoalls(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                      uint64_t src_off, int64_t dst, int64_t sst, uint64_t nelems,
+                      uint64_t elem_size, void *stream) {
+  int rc = alltoalls_launch(pe_start, pe_stride, pe_size, dest_off, src_off, dst, sst, nelems,
+                            elem_size, pick_stream(stream));
+  return rc ? rc : finish(stream, "b200shm_alltoalls");
+}
+
+int b200shm_broadcast(int root, int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                      uint64_t src_off, uint64_t nbytes, void *stream) {
+  int rc = broadcast_launch(root, pe_start, pe_stride, pe_size, dest_off, src_off, nbytes,
+                            pick_stream(stream));
+  return rc ? rc : finish(stream, "b200shm_broadcast");
+}
+
+}  // extern "C"

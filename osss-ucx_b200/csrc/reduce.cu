@@ -1,0 +1,615 @@
+/*
+ * reduce.cu -- one-pass all-reduce over the members of a team.
+ *
+ * The reference moves O(N log P) bytes per PE through log2(P) rounds of
+ * put + flag handshake (rec_dbl, src/shcoll/src/reduce.c:182-293) or
+ * reduce-scatter + allgather (Rabenseifner, 306-724).  On one GPU every
+ * member's slice is directly addressable, so each thread owns a 16-byte
+ * column of elements, streams that column in from all P members' sources
+ * with 128-bit loads, combines it in registers and streams the result out
+ * to all P members' dests: 2*P*N*sizeof(T) bytes, the algorithmic minimum.
+ *
+ * Exactness.  The algorithm fixes the combine order and so the exact
+ * floating-point result.  Three facts keep the kernel cheap:
+ *  - integer AND/OR/XOR/SUM/PROD (wrapping) and MIN/MAX are associative
+ *    and commutative bit for bit, so any order is exact: a running chain;
+ *  - float and complex SUM/PROD are exactly commutative (a+b == b+a, and
+ *    the naive complex product is symmetric), so only the tree SHAPE
+ *    matters: linear = left fold (reduce.c:78-81); binomial = balanced
+ *    binary tree over members combining op(upper block, lower block)
+ *    (reduce.c:137-154, children in increasing mask order); rec_dbl and
+ *    both Rabenseifner variants = butterfly over the power-of-two subset
+ *    after folding the extra members (reduce.c:206-272, 338-454) -- the
+ *    same tree for all three;
+ *  - float MIN/MAX written a<b?a:b (reduce.c:731-732) is order dependent
+ *    only when the operands include a NaN or both +0 and -0; elements with
+ *    such operands take an exact per-member path that replays the
+ *    algorithm's operand order (rec_dbl then gives different members
+ *    different bits, exactly as the reference does).
+ * Trees are evaluated as a binary counter over the leaves, with one
+ * register slot per tree level, so leaves stream in member order.
+ * No fused multiply-add is ever formed: float ops use the _rn intrinsics.
+ */
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace b200 {
+namespace {
+
+struct cf32 {
+  float re, im;
+};
+struct cf64 {
+  double re, im;
+};
+
+enum { ORD_CHAIN = 0, ORD_BINOMIAL = 1, ORD_BUTTERFLY = 2 };
+
+/* ---- element operators (reduce.c:730-736) ------------------------------ */
+template <int OP, class T>
+__device__ __forceinline__ T op_int(T a, T b) {
+  typedef typename std::make_unsigned<T>::type U;
+  if constexpr (OP == B200SHM_AND) return (T)(a & b);
+  else if constexpr (OP == B200SHM_OR) return (T)(a | b);
+  else if constexpr (OP == B200SHM_XOR) return (T)(a ^ b);
+  else if constexpr (OP == B200SHM_MIN) return a < b ? a : b;
+  else if constexpr (OP == B200SHM_MAX) return a > b ? a : b;
+  else if constexpr (OP == B200SHM_SUM) return (T)(U)((uint64_t)(U)a + (uint64_t)(U)b);
+  else return (T)(U)((uint64_t)(U)a * (uint64_t)(U)b);
+}
+
+__device__ __forceinline__ float f_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float f_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float f_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double f_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double f_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double f_sub(double a, double b) { return __dsub_rn(a, b); }
+
+template <int OP, class F>
+__device__ __forceinline__ F op_flt(F a, F b) {
+  if constexpr (OP == B200SHM_MIN) return a < b ? a : b;
+  else if constexpr (OP == B200SHM_MAX) return a > b ? a : b;
+  else if constexpr (OP == B200SHM_SUM) return f_add(a, b);
+  else return f_mul(a, b);
+}
+
+/* Complex product as C99 evaluates x*y: the naive formula, and only when
+ * both parts come out NaN, the infinity recovery of ISO C Annex G.5.1
+ * (what the reference's gcc build reaches through __muldc3/__mulsc3). */
+template <class F>
+__device__ __forceinline__ F cpy_sign(F mag, F sgn) { return copysign(mag, sgn); }
+template <class F>
+__device__ void cmul(F a, F b, F c, F d, F &re, F &im) {
+  F ac = f_mul(a, c), bd = f_mul(b, d), ad = f_mul(a, d), bc = f_mul(b, c);
+  re = f_sub(ac, bd);
+  im = f_add(ad, bc);
+  if (isnan(re) && isnan(im)) {
+    bool recalc = false;
+    if (isinf(a) || isinf(b)) {
+      a = cpy_sign((F)(isinf(a) ? 1 : 0), a);
+      b = cpy_sign((F)(isinf(b) ? 1 : 0), b);
+      if (isnan(c)) c = cpy_sign((F)0, c);
+      if (isnan(d)) d = cpy_sign((F)0, d);
+      recalc = true;
+    }
+    if (isinf(c) || isinf(d)) {
+      c = cpy_sign((F)(isinf(c) ? 1 : 0), c);
+      d = cpy_sign((F)(isinf(d) ? 1 : 0), d);
+      if (isnan(a)) a = cpy_sign((F)0, a);
+      if (isnan(b)) b = cpy_sign((F)0, b);
+      recalc = true;
+    }
+    if (!recalc && (isinf(ac) || isinf(bd) || isinf(ad) || isinf(bc))) {
+      if (isnan(a)) a = cpy_sign((F)0, a);
+      if (isnan(b)) b = cpy_sign((F)0, b);
+      if (isnan(c)) c = cpy_sign((F)0, c);
+      if (isnan(d)) d = cpy_sign((F)0, d);
+      recalc = true;
+    }
+    if (recalc) {
+      const F inf = (F)INFINITY;
+      re = f_mul(inf, f_sub(f_mul(a, c), f_mul(b, d)));
+      im = f_mul(inf, f_add(f_mul(a, d), f_mul(b, c)));
+    }
+  }
+}
+
+template <int OP, class T>
+__device__ __forceinline__ T apply(T a, T b) {
+  if constexpr (std::is_same<T, float>::value || std::is_same<T, double>::value) {
+    return op_flt<OP>(a, b);
+  } else if constexpr (std::is_same<T, cf32>::value || std::is_same<T, cf64>::value) {
+    T r;
+    if constexpr (OP == B200SHM_SUM) {
+      r.re = f_add(a.re, b.re);
+      r.im = f_add(a.im, b.im);
+    } else {
+      cmul(a.re, a.im, b.re, b.im, r.re, r.im);
+    }
+    return r;
+  } else {
+    return op_int<OP>(a, b);
+  }
+}
+
+/* ---- packs: V consecutive elements moved as one 16-byte access -------- */
+template <class T, int V>
+struct alignas(V * sizeof(T) >= 16 ? 16 : alignof(T)) Pack {
+  T x[V];
+};
+
+template <class T, int V>
+__device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
+  Pack<T, V> r;
+  if constexpr (sizeof(Pack<T, V>) == 16) {
+    uint4 u;
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+        : "=r"(u.x), "=r"(u.y), "=r"(u.z), "=r"(u.w)
+        : "l"(p));
+    memcpy(&r, &u, 16);
+  } else {
+    memcpy(&r, p, sizeof(r));
+  }
+  return r;
+}
+template <class T, int V>
+__device__ __forceinline__ void st_pack(char *p, const Pack<T, V> &v) {
+  if constexpr (sizeof(Pack<T, V>) == 16) {
+    uint4 u;
+    memcpy(&u, &v, 16);
+    asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y),
+                 "r"(u.z), "r"(u.w)
+                 : "memory");
+  } else {
+    memcpy(p, &v, sizeof(v));
+  }
+}
+template <int OP, class T, int V>
+__device__ __forceinline__ Pack<T, V> papply(const Pack<T, V> &a, const Pack<T, V> &b) {
+  Pack<T, V> r;
+#pragma unroll
+  for (int i = 0; i < V; i++) r.x[i] = apply<OP>(a.x[i], b.x[i]);
+  return r;
+}
+
+/* MIN/MAX on floats: flag bit 0 = NaN seen, bit 1 = +0 seen, bit 2 = -0. */
+__device__ __forceinline__ unsigned fclass(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return ((u & 0x7fffffffu) > 0x7f800000u ? 1u : 0u) | (u == 0u ? 2u : 0u) |
+         (u == 0x80000000u ? 4u : 0u);
+}
+__device__ __forceinline__ unsigned fclass(double f) {
+  const uint64_t u = (uint64_t)__double_as_longlong(f);
+  return ((u & 0x7fffffffffffffffull) > 0x7ff0000000000000ull ? 1u : 0u) |
+         (u == 0ull ? 2u : 0u) | (u == 0x8000000000000000ull ? 4u : 0u);
+}
+__device__ __forceinline__ bool ambiguous(unsigned f) { return (f & 1u) || (f & 6u) == 6u; }
+
+struct RArgs {
+  const char *src;  /* member 0's source at element 0          */
+  char *dst;        /* member 0's dest at element 0            */
+  uint64_t sstep;   /* bytes from member i to member i+1 (src) */
+  uint64_t dstep;   /* same for dest (equal; kept separate)    */
+  uint64_t e_begin; /* first element of this launch            */
+  uint64_t nvec;    /* packs in this launch                    */
+  uint64_t N;       /* elements of the whole reduction         */
+  int P, p2s, logp2s, algo;
+  unsigned long long *fix_list, *fix_count; /* deferred elements */
+  unsigned long long fix_cap;
+  int *status;
+};
+
+/* p2s membership, reduce.c:206-214 and 232 */
+__device__ __forceinline__ int p2s_member(int q, int P, int p2s) {
+  return (int)(((long long)q * P + p2s - 1) / p2s);
+}
+__device__ __forceinline__ bool p2s_extra(int q, int P, int p2s) {
+  const int as = p2s_member(q, P, p2s);
+  return (long long)(as + 1) * p2s / P == q;
+}
+
+constexpr int kMaxLevels = 13; /* trees of up to 4096 leaves */
+
+/* ---- exact replay for order-dependent MIN/MAX elements ----------------- */
+/* Value the algorithm leaves in p2s member q's dest (rec_dbl), or in every
+ * member's dest (the other algorithms, q = block owner or 0), for one
+ * element whose P inputs are vals[0..P). */
+template <class T, int OP>
+__device__ T exact_value(const T *vals, int P, int p2s, int logp2s, int algo, bool lower_half,
+                         int q) {
+  if (algo == B200SHM_LINEAR) {
+    T acc = vals[0];
+    for (int j = 1; j < P; j++) acc = apply<OP>(acc, vals[j]);
+    return acc;
+  }
+  T stk[kMaxLevels + 1];
+  if (algo == B200SHM_BINOMIAL) {
+    for (int j = 0; j < P; j++) {
+      T x = vals[j];
+      for (int L = 0; L <= kMaxLevels; L++) {
+        if (j & (1 << L)) {
+          x = apply<OP>(x, stk[L]); /* op(upper block, lower block) */
+        } else {
+          stk[L] = x;
+          break;
+        }
+      }
+    }
+    bool have = false;
+    T v = stk[0];
+    for (int L = 0; L <= kMaxLevels; L++)
+      if (P & (1 << L)) {
+        v = have ? apply<OP>(v, stk[L]) : stk[L];
+        have = true;
+      }
+    return v;
+  }
+  /* butterfly: rec_dbl / rabenseifner / rabenseifner2 */
+  const bool rab = algo != B200SHM_REC_DBL;
+  for (int leaf = 0; leaf < p2s; leaf++) {
+    const int as = p2s_member(leaf, P, p2s);
+    T x = vals[as];
+    if (p2s_extra(leaf, P, p2s)) {
+      const T ext = vals[as + 1];
+      /* rec_dbl: op(extra, own) (reduce.c:241); Rabenseifner: op(extra,
+       * own) on the lower half (397), op(own, extra) on the upper (375) */
+      x = (!rab || lower_half) ? apply<OP>(ext, x) : apply<OP>(x, ext);
+    }
+    for (int L = 0; L <= kMaxLevels; L++) {
+      if (leaf & (1 << L)) {
+        /* member q computes op(own, partner's) (reduce.c:268, 448) */
+        x = (q & (1 << L)) ? apply<OP>(x, stk[L]) : apply<OP>(stk[L], x);
+      } else {
+        stk[L] = x;
+        break;
+      }
+    }
+  }
+  return stk[logp2s];
+}
+
+/* Block of element e in Rabenseifner's split: [b*N/p2s, (b+1)*N/p2s). */
+__device__ int rab_block(uint64_t e, uint64_t N, int p2s) {
+  int b = (int)((e * (uint64_t)p2s) / (N ? N : 1));
+  if (b >= p2s) b = p2s - 1;
+  while (b + 1 < p2s && (uint64_t)(b + 1) * N / (uint64_t)p2s <= e) b++;
+  while (b > 0 && (uint64_t)b * N / (uint64_t)p2s > e) b--;
+  return b;
+}
+__device__ __forceinline__ int rev_bits(int x, int n) {
+  return n ? (int)(__brev((unsigned)x) >> (32 - n)) : 0;
+}
+
+constexpr int kFixMaxMembers = 4096;
+
+/* Second pass over the elements the streaming kernel deferred (it left
+ * their dests untouched, so in-place sources are still intact): one CTA
+ * per element stages the P inputs in shared memory, then replays the
+ * algorithm's operand order from there. */
+template <class T, int OP>
+__global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
+                                                    const unsigned long long *list,
+                                                    const unsigned long long *count,
+                                                    unsigned long long cap) {
+  __shared__ T vals[kFixMaxMembers];
+  __shared__ T common;
+  const unsigned long long n = *count < cap ? *count : cap;
+  for (unsigned long long k = blockIdx.x; k < n; k += gridDim.x) {
+    const uint64_t e = list[k];
+    for (int j = threadIdx.x; j < a.P; j += blockDim.x)
+      memcpy(&vals[j], a.src + (uint64_t)j * a.sstep + e * sizeof(T), sizeof(T));
+    __syncthreads();
+    const bool lower = e < a.N / 2;
+    if (a.algo == B200SHM_REC_DBL) {
+      /* every p2s member (and the extra folded into it) keeps its own value */
+      for (int q = threadIdx.x; q < a.p2s; q += blockDim.x) {
+        const T v = exact_value<T, OP>(vals, a.P, a.p2s, a.logp2s, a.algo, lower, q);
+        const int as = p2s_member(q, a.P, a.p2s);
+        memcpy(a.dst + (uint64_t)as * a.dstep + e * sizeof(T), &v, sizeof(T));
+        if (p2s_extra(q, a.P, a.p2s))
+          memcpy(a.dst + (uint64_t)(as + 1) * a.dstep + e * sizeof(T), &v, sizeof(T));
+      }
+    } else {
+      if (threadIdx.x == 0) {
+        int q = 0;
+        if (a.algo != B200SHM_LINEAR && a.algo != B200SHM_BINOMIAL)
+          q = rev_bits(rab_block(e, a.N, a.p2s), a.logp2s); /* owner of e's block */
+        common = exact_value<T, OP>(vals, a.P, a.p2s, a.logp2s, a.algo, lower, q);
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < a.P; j += blockDim.x)
+        memcpy(a.dst + (uint64_t)j * a.dstep + e * sizeof(T), &common, sizeof(T));
+    }
+    __syncthreads();
+  }
+}
+
+/* ---- the streaming kernels -------------------------------------------- */
+template <class T, int OP, int ORDER, int V, int U, bool MINMAX_CHECK, int LV>
+__global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
+  typedef Pack<T, V> PK;
+  const uint64_t gstride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.nvec; v += gstride) {
+    const uint64_t e0 = a.e_begin + v * V;
+    const char *src = a.src + e0 * sizeof(T);
+    PK r;
+    unsigned cls[V];
+    if constexpr (ORDER == ORD_CHAIN) {
+      r = ld_pack<T, V>(src);
+      if constexpr (MINMAX_CHECK) {
+#pragma unroll
+        for (int i = 0; i < V; i++) cls[i] = fclass(r.x[i]);
+      }
+      for (int j = 1; j < a.P; j += U) {
+        PK x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (j + u < a.P) x[u] = ld_pack<T, V>(src + (uint64_t)(j + u) * a.sstep);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (j + u < a.P) {
+            r = papply<OP>(r, x[u]);
+            if constexpr (MINMAX_CHECK) {
+#pragma unroll
+              for (int i = 0; i < V; i++) cls[i] |= fclass(x[u].x[i]);
+            }
+          }
+      }
+    } else {
+      PK stk[LV]; /* LV levels hold trees of up to 2^LV - 1 leaves */
+      const int nleaves = ORDER == ORD_BUTTERFLY ? a.p2s : a.P;
+      for (int q0 = 0; q0 < nleaves; q0 += U) {
+        PK x[U];
+        if constexpr (ORDER == ORD_BUTTERFLY) {
+#pragma unroll
+          for (int u = 0; u < U; u++)
+            if (q0 + u < nleaves)
+              x[u] = ld_pack<T, V>(src + (uint64_t)p2s_member(q0 + u, a.P, a.p2s) * a.sstep);
+          if (a.P != a.p2s) {
+            /* fold the extra member into its p2s partner: op(extra, own) */
+#pragma unroll
+            for (int u = 0; u < U; u++)
+              if (q0 + u < nleaves && p2s_extra(q0 + u, a.P, a.p2s)) {
+                const int as = p2s_member(q0 + u, a.P, a.p2s);
+                x[u] = papply<OP>(ld_pack<T, V>(src + (uint64_t)(as + 1) * a.sstep), x[u]);
+              }
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; u++)
+            if (q0 + u < nleaves) x[u] = ld_pack<T, V>(src + (uint64_t)(q0 + u) * a.sstep);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (q0 + u < nleaves) {
+            /* binary counter: leaf q closes t = trailing_ones(q) blocks, then
+             * parks the merged block at level t (static register indices) */
+            const int q = q0 + u;
+            const int t = __ffs(~q) - 1;
+            PK y = x[u];
+#pragma unroll
+            for (int L = 0; L < LV - 1; L++)
+              if (L < t) y = ORDER == ORD_BUTTERFLY ? papply<OP>(stk[L], y) : papply<OP>(y, stk[L]);
+#pragma unroll
+            for (int L = 0; L < LV; L++)
+              if (L == t) stk[L] = y;
+          }
+        }
+      }
+      if constexpr (ORDER == ORD_BUTTERFLY) {
+#pragma unroll
+        for (int L = 0; L < LV; L++)
+          if (L == a.logp2s) r = stk[L];
+      } else {
+        bool have = false;
+#pragma unroll
+        for (int L = 0; L < LV; L++)
+          if (a.P & (1 << L)) {
+            r = have ? papply<OP>(r, stk[L]) : stk[L];
+            have = true;
+          }
+      }
+    }
+    if constexpr (MINMAX_CHECK) {
+      bool amb = false;
+#pragma unroll
+      for (int i = 0; i < V; i++) amb |= ambiguous(cls[i]);
+      if (amb) {
+        /* defer the whole pack; its dests stay untouched until k_minmax_fix */
+        const unsigned long long slot = atomicAdd(a.fix_count, (unsigned long long)V);
+        for (int i = 0; i < V; i++) {
+          if (slot + i < a.fix_cap) a.fix_list[slot + i] = e0 + i;
+          else atomicOr(a.status, (int)B200SHM_STATUS_FIX_OVERFLOW);
+        }
+        continue;
+      }
+    }
+    char *dst = a.dst + e0 * sizeof(T);
+    for (int j = 0; j < a.P; j++) st_pack<T, V>(dst + (uint64_t)j * a.dstep, r);
+  }
+}
+
+/* Launch the packed body over [0, N - N%V) and a scalar tail, or scalar
+ * throughout when the buffers are not 16-byte aligned. */
+template <class T, int OP, int ORDER, bool MM, int LV>
+void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
+  constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
+  constexpr int U = ORDER == ORD_CHAIN ? 8 : 4;
+  RArgs a = base;
+  uint64_t done = 0;
+  if (aligned && V > 1) {
+    a.e_begin = 0;
+    a.nvec = base.N / V;
+    if (a.nvec) {
+      k_reduce<T, OP, ORDER, V, U, MM, LV><<<grid_for(a.nvec, 256, 8), 256, 0, s>>>(a);
+      count_launch();
+      done = a.nvec * V;
+    }
+  }
+  if (done < base.N) {
+    a.e_begin = done;
+    a.nvec = base.N - done;
+    k_reduce<T, OP, ORDER, 1, U, MM, LV><<<grid_for(a.nvec, 256, 8), 256, 0, s>>>(a);
+    count_launch();
+  }
+}
+
+template <class T, int OP, int ORDER, bool MM>
+int run(const RArgs &base, bool aligned, cudaStream_t s) {
+  if constexpr (ORDER == ORD_CHAIN) {
+    run_lv<T, OP, ORDER, MM, 1>(base, aligned, s);
+  } else {
+    const int leaves = ORDER == ORD_BUTTERFLY ? base.p2s : base.P;
+    if (leaves < (1 << 8))
+      run_lv<T, OP, ORDER, MM, 8>(base, aligned, s);
+    else
+      run_lv<T, OP, ORDER, MM, kMaxLevels>(base, aligned, s);
+  }
+  if constexpr (MM) {
+    k_minmax_fix<T, OP><<<2 * st().sm_count, 256, 0, s>>>(base, base.fix_list, base.fix_count,
+                                                         base.fix_cap);
+    count_launch();
+  }
+  return B200SHM_OK;
+}
+
+template <class T, int OP>
+int run_float(const RArgs &a, bool aligned, cudaStream_t s) {
+  if constexpr (OP == B200SHM_MIN || OP == B200SHM_MAX) {
+    B200_CK(cudaMemsetAsync(a.fix_count, 0, sizeof(unsigned long long), s));
+    return run<T, OP, ORD_CHAIN, true>(a, aligned, s);
+  } else {
+    switch (a.algo) {
+    case B200SHM_LINEAR: return run<T, OP, ORD_CHAIN, false>(a, aligned, s);
+    case B200SHM_BINOMIAL: return run<T, OP, ORD_BINOMIAL, false>(a, aligned, s);
+    default: return run<T, OP, ORD_BUTTERFLY, false>(a, aligned, s);
+    }
+  }
+}
+
+template <class T, int OP>
+int run_cplx(const RArgs &a, bool aligned, cudaStream_t s) {
+  switch (a.algo) {
+  case B200SHM_LINEAR: return run<T, OP, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_BINOMIAL: return run<T, OP, ORD_BINOMIAL, false>(a, aligned, s);
+  default: return run<T, OP, ORD_BUTTERFLY, false>(a, aligned, s);
+  }
+}
+
+/* Integer ops other than MIN/MAX give the same bits on signed and unsigned
+ * views, so they run on the unsigned type of the same width. */
+template <class S, class U>
+int run_int(int op, const RArgs &a, bool aligned, cudaStream_t s) {
+  switch (op) {
+  case B200SHM_AND: return run<U, B200SHM_AND, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_OR: return run<U, B200SHM_OR, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_XOR: return run<U, B200SHM_XOR, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_MIN: return run<S, B200SHM_MIN, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_MAX: return run<S, B200SHM_MAX, ORD_CHAIN, false>(a, aligned, s);
+  case B200SHM_SUM: return run<U, B200SHM_SUM, ORD_CHAIN, false>(a, aligned, s);
+  default: return run<U, B200SHM_PROD, ORD_CHAIN, false>(a, aligned, s);
+  }
+}
+
+}  // namespace
+
+static const int kDtypeSize[B200SHM_NDTYPE] = {1, 2, 4, 8, 1, 2, 4, 8, 4, 8, 16, 8, 16};
+
+/* Host side of b200shm_reduce, also used by the batched and serving paths. */
+int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
+                  uint64_t dest_off, uint64_t src_off, uint64_t nelems, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, pe_size);
+  if (rc) return rc;
+  if (op < 0 || op >= B200SHM_NOP || dtype < 0 || dtype >= B200SHM_NDTYPE || algo < 0 ||
+      algo >= B200SHM_NALGO)
+    return fail(B200SHM_ERR_ARG, "reduce: bad op %d / dtype %d / algo %d", op, dtype, algo);
+  const bool is_int = dtype <= B200SHM_U64;
+  const bool is_cpx = dtype == B200SHM_C32 || dtype == B200SHM_C64;
+  if ((op <= B200SHM_XOR && !is_int) || ((op == B200SHM_MIN || op == B200SHM_MAX) && is_cpx))
+    return fail(B200SHM_ERR_UNSUPPORTED, "reduce: op %d is not defined on dtype %d", op, dtype);
+  if (dtype == B200SHM_F80)
+    return fail(B200SHM_ERR_UNSUPPORTED,
+                "reduce: long double (x87 80-bit) arithmetic is not available on the GPU");
+  const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  if (nelems > st().slice / es) return fail(B200SHM_ERR_ARG, "reduce: nelems too large");
+  const uint64_t bytes = nelems * es;
+  if ((rc = check_extent(src_off, bytes, "reduce source"))) return rc;
+  if ((rc = check_extent(dest_off, bytes, "reduce dest"))) return rc;
+  if (dest_off != src_off && overlaps(dest_off, bytes, src_off, bytes))
+    return fail(B200SHM_ERR_ARG, "reduce: dest and source overlap without being identical");
+  if (nelems == 0) return B200SHM_OK;
+  int logp = 0, p2s = 1;
+  while (p2s * 2 <= pe_size) {
+    p2s *= 2;
+    logp++;
+  }
+  const bool tree = !is_int && op != B200SHM_MIN && op != B200SHM_MAX && algo != B200SHM_LINEAR;
+  const int leaves = algo == B200SHM_BINOMIAL ? pe_size : p2s;
+  if (tree && leaves > (1 << (kMaxLevels - 1)))
+    return fail(B200SHM_ERR_UNSUPPORTED, "reduce: float combine trees are limited to %d members",
+                1 << (kMaxLevels - 1));
+  if (!is_int && (op == B200SHM_MIN || op == B200SHM_MAX) && pe_size > kFixMaxMembers)
+    return fail(B200SHM_ERR_UNSUPPORTED, "reduce: float MIN/MAX is limited to %d members",
+                kFixMaxMembers);
+  Members m = members(pe_start, pe_stride, pe_size);
+  RArgs a;
+  a.src = m.first + src_off;
+  a.dst = m.first + dest_off;
+  a.sstep = a.dstep = m.step;
+  a.e_begin = 0;
+  a.nvec = 0;
+  a.N = nelems;
+  a.P = pe_size;
+  a.p2s = p2s;
+  a.logp2s = logp;
+  a.algo = algo;
+  a.fix_list = st().fix_list;
+  a.fix_count = st().fix_count;
+  a.fix_cap = st().fix_cap;
+  a.status = st().d_status;
+  const bool aligned = ((src_off | dest_off | m.step) & 15u) == 0;
+  switch (dtype) {
+  case B200SHM_I8: return run_int<int8_t, uint8_t>(op, a, aligned, s);
+  case B200SHM_I16: return run_int<int16_t, uint16_t>(op, a, aligned, s);
+  case B200SHM_I32: return run_int<int32_t, uint32_t>(op, a, aligned, s);
+  case B200SHM_I64: return run_int<int64_t, uint64_t>(op, a, aligned, s);
+  case B200SHM_U8: return run_int<uint8_t, uint8_t>(op, a, aligned, s);
+  case B200SHM_U16: return run_int<uint16_t, uint16_t>(op, a, aligned, s);
+  case B200SHM_U32: return run_int<uint32_t, uint32_t>(op, a, aligned, s);
+  case B200SHM_U64: return run_int<uint64_t, uint64_t>(op, a, aligned, s);
+  case B200SHM_F32:
+    switch (op) {
+    case B200SHM_MIN: return run_float<float, B200SHM_MIN>(a, aligned, s);
+    case B200SHM_MAX: return run_float<float, B200SHM_MAX>(a, aligned, s);
+    case B200SHM_SUM: return run_float<float, B200SHM_SUM>(a, aligned, s);
+    default: return run_float<float, B200SHM_PROD>(a, aligned, s);
+    }
+  case B200SHM_F64:
+    switch (op) {
+    case B200SHM_MIN: return run_float<double, B200SHM_MIN>(a, aligned, s);
+    case B200SHM_MAX: return run_float<double, B200SHM_MAX>(a, aligned, s);
+    case B200SHM_SUM: return run_float<double, B200SHM_SUM>(a, aligned, s);
+    default: return run_float<double, B200SHM_PROD>(a, aligned, s);
+    }
+  case B200SHM_C32:
+    return op == B200SHM_SUM ? run_cplx<cf32, B200SHM_SUM>(a, aligned, s)
+                             : run_cplx<cf32, B200SHM_PROD>(a, aligned, s);
+  default:
+    return op == B200SHM_SUM ? run_cplx<cf64, B200SHM_SUM>(a, aligned, s)
+                             : run_cplx<cf64, B200SHM_PROD>(a, aligned, s);
+  }
+}
+
+}  // namespace b200
+
+extern "C" int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_stride,
+                              int pe_size, uint64_t dest_off, uint64_t src_off, uint64_t nelems,
+                              void *stream) {
+  int rc = b200::reduce_launch(op, dtype, algo, pe_start, pe_stride, pe_size, dest_off, src_off,
+                               nelems, b200::pick_stream(stream));
+  if (rc) return rc;
+  return b200::finish(stream, "b200shm_reduce");
+}

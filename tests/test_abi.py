@@ -1,0 +1,41 @@
+"""The C ABI library loads on any machine and exports every entry point its
+public headers declare; without a GPU every compute call fails cleanly."""
+import ctypes
+import os
+import re
+
+import b200shm
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", h) for h in sorted(os.listdir(os.path.join(ROOT, "include")))
+           if h.startswith("b200shm") and h.endswith(".h")]
+
+
+def declared(header):
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(b200shm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    assert HEADERS
+    lib = ctypes.CDLL(b200shm.LIB_PATH)
+    missing = []
+    for h in HEADERS:
+        for name in declared(h):
+            try:
+                getattr(lib, name)
+            except AttributeError:
+                missing.append((os.path.basename(h), name))
+    assert not missing, missing
+
+
+def test_calls_before_init_fail_with_state_error():
+    L = b200shm.lib
+    if L.b200shm_initialized():
+        return  # a GPU session already initialised the engine in this process
+    rc = L.b200shm_reduce(5, 8, 2, 0, 1, 4, 0, 0, 16, None)
+    assert rc == -5 and b"not initialised" in L.b200shm_last_error()
+    assert L.b200shm_fcollect(0, 1, 4, 0, 0, 64, None) == -5
+    assert L.b200shm_barrier(2, 0, 1, 4, None) == -5
+    assert L.b200shm_ptr(0, 0) is None
