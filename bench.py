@@ -47,7 +47,7 @@ FALLBACK_HBM = 6650.0
 
 
 def workload_desc(n_gpus):
-    return {"workload": "allreduce over 64 emulated PEs x 2^20 elems/PE: f32 sum N(0,1), "
+    return {"workload": f"allreduce over 64 emulated PEs x {N} elems/PE: f32 sum N(0,1), "
                         "f64 max U(-1e6,1e6), i64 xor U(bits); rec_dbl and rabenseifner orders",
             "npes": P, "nelems_per_pe": N, "heap_bytes": P * HEAP,
             "ops": [f"{d}:{o}" for o, d, _ in OPS], "algos": ALGOS,
@@ -55,11 +55,12 @@ def workload_desc(n_gpus):
             "parallelism": f"{n_gpus} independent 64-PE teams, one per GPU"}
 
 
-def inputs(seed_base=0):
+def inputs(seed_base=0, which=(0, 1, 2)):
     import gen
-    return [gen.normal(np.float32, P, N, 21 + seed_base),
-            gen.uniform(np.float64, P, N, 22 + seed_base, -1e6, 1e6),
-            gen.uniform_int(np.int64, P, N, 23 + seed_base)]
+    make = [lambda: gen.normal(np.float32, P, N, 21 + seed_base),
+            lambda: gen.uniform(np.float64, P, N, 22 + seed_base, -1e6, 1e6),
+            lambda: gen.uniform_int(np.int64, P, N, 23 + seed_base)]
+    return [make[i]() if i in which else None for i in range(3)]
 
 
 def alg_bytes(npes, n, dt):
@@ -195,6 +196,7 @@ def run_reference_arm(args, rank):
 # GPU
 # ---------------------------------------------------------------------------
 def main():
+    global N
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -202,6 +204,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", action="append", default=[],
+                    help="time only dtype:op:algo (repeatable), e.g. float32:sum:rec_dbl")
+    ap.add_argument("--heap-mb", type=int, default=HEAP >> 20, help="heap slice per PE (MiB)")
+    ap.add_argument("--nelems", type=int, default=N, help="elements per PE")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -224,22 +230,28 @@ def main():
     import __graft_entry__
     __graft_entry__.build_library()
     import b200shm as B
-    B.init(P, HEAP)
+    N = args.nelems
+    B.init(P, args.heap_mb << 20)
     team = (0, 1, P)
-    xs = inputs(seed_base=rank * 100)
-    src, dst = B.malloc(8 * N), B.malloc(8 * N)
-    srcs = []
-    for x in xs:
-        off = B.malloc(x[0].nbytes)
-        B.put_rows(off, x, team=team)
-        srcs.append(off)
+    calls = [(op, dt, algo, i, npdt) for i, (op, dt, npdt) in enumerate(OPS) for algo in ALGOS]
+    if args.case:
+        calls = [c for c in calls if f"{c[1]}:{c[0]}:{c[2]}" in args.case]
+        if not calls:
+            raise SystemExit("no reduction matches --case " + ",".join(args.case))
+    used = sorted({c[3] for c in calls})
+    xs = inputs(seed_base=rank * 100, which=used)
+    dst = B.malloc(max(xs[i][0].nbytes for i in used))
+    srcs = [None] * 3
+    for i in used:
+        srcs[i] = B.malloc(xs[i][0].nbytes)
+        B.put_rows(srcs[i], xs[i], team=team)
+    calls = [(op, dt, algo, srcs[i], npdt, i) for op, dt, algo, i, npdt in calls]
     stream_ptr = B.stream()
     s = torch.cuda.ExternalStream(stream_ptr)
-    calls = [(op, dt, algo, srcs[i], npdt) for i, (op, dt, npdt) in enumerate(OPS) for algo in ALGOS]
     step_bytes = sum(alg_bytes(P, N, c[4]) for c in calls)
 
     def step(evs=None):
-        for j, (op, dt, algo, so, _) in enumerate(calls):
+        for j, (op, dt, algo, so, _, _) in enumerate(calls):
             if evs is not None:
                 evs[j][0].record(s)
             B.reduce(op, dt, algo, dst, so, N, team=team, stream=stream_ptr)
@@ -281,7 +293,7 @@ def main():
 
     # per-kernel durations (the reduce kernel of each (dtype, op, order))
     durs = {}
-    for j, (op, dt, algo, _, npdt) in enumerate(calls):
+    for j, (op, dt, algo, _, npdt, _) in enumerate(calls):
         d = [per_call[k][j][0].elapsed_time(per_call[k][j][1]) for k in range(args.steps)]
         durs[f"{dt}:{op}:{algo}"] = (float(np.mean(d)), alg_bytes(P, N, npdt))
     dom = max(durs, key=lambda k: durs[k][0])
@@ -297,21 +309,21 @@ def main():
     # e2e: host buffers in, reduce, host buffers out, through the C ABI
     e2e = None
     if args.e2e_steps > 0:
-        pinned_in = [torch.from_numpy(x).pin_memory() for x in xs]
-        pinned_out = [torch.empty(x.shape, dtype=torch.from_numpy(x[:1]).dtype).pin_memory() for x in xs]
+        pinned_in = {i: torch.from_numpy(xs[i]).pin_memory() for i in used}
+        pinned_out = {i: torch.empty(xs[i].shape, dtype=pinned_in[i].dtype).pin_memory()
+                      for i in used}
         h2d = d2h = 0
 
         def e2e_step():
             nonlocal h2d, d2h
             h2d = d2h = 0
-            for i, (op, dt, npdt) in enumerate(OPS):
-                for algo in ALGOS:
-                    nb = xs[i][0].nbytes
-                    B.lib.b200shm_put_host(0, 1, P, srcs[i], pinned_in[i].data_ptr(), nb, stream_ptr)
-                    B.reduce(op, dt, algo, dst, srcs[i], N, team=team, stream=stream_ptr)
-                    B.lib.b200shm_get_host(pinned_out[i].data_ptr(), 0, 1, P, dst, nb, stream_ptr)
-                    h2d += P * nb
-                    d2h += P * nb
+            for op, dt, algo, so, npdt, i in calls:
+                nb = xs[i][0].nbytes
+                B.lib.b200shm_put_host(0, 1, P, so, pinned_in[i].data_ptr(), nb, stream_ptr)
+                B.reduce(op, dt, algo, dst, so, N, team=team, stream=stream_ptr)
+                B.lib.b200shm_get_host(pinned_out[i].data_ptr(), 0, 1, P, dst, nb, stream_ptr)
+                h2d += P * nb
+                d2h += P * nb
         e2e_step()
         B.quiet()
         barrier()

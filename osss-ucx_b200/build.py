@@ -50,6 +50,9 @@ def build(verbose=False, extra=()):
     os.makedirs(LIB, exist_ok=True)
     heads = _headers()
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    lib = os.path.join(LIB, CUDA_LIB)
+    if not extra and not _stale(lib, srcs + heads + [__file__]):
+        return lib  # up to date (objects may be absent, e.g. in a shipped snapshot)
     jobs = []
     objs = []
     for s in srcs:
@@ -61,7 +64,6 @@ def build(verbose=False, extra=()):
         for o in ex.map(lambda so: _compile(so[0], so[1], extra), jobs):
             if verbose:
                 print("compiled", o)
-    lib = os.path.join(LIB, CUDA_LIB)
     if _stale(lib, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)

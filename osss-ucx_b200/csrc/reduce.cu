@@ -31,6 +31,8 @@
  * No fused multiply-add is ever formed: float ops use the _rn intrinsics.
  */
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <type_traits>
 
@@ -217,18 +219,17 @@ constexpr int kMaxLevels = 13; /* trees of up to 4096 leaves */
 /* Value the algorithm leaves in p2s member q's dest (rec_dbl), or in every
  * member's dest (the other algorithms, q = block owner or 0), for one
  * element whose P inputs are vals[0..P). */
-template <class T, int OP>
-__device__ T exact_value(const T *vals, int P, int p2s, int logp2s, int algo, bool lower_half,
-                         int q) {
+template <class T, int OP, class Get>
+__device__ T exact_value(Get vals, int P, int p2s, int logp2s, int algo, bool lower_half, int q) {
   if (algo == B200SHM_LINEAR) {
-    T acc = vals[0];
-    for (int j = 1; j < P; j++) acc = apply<OP>(acc, vals[j]);
+    T acc = vals(0);
+    for (int j = 1; j < P; j++) acc = apply<OP>(acc, vals(j));
     return acc;
   }
   T stk[kMaxLevels + 1];
   if (algo == B200SHM_BINOMIAL) {
     for (int j = 0; j < P; j++) {
-      T x = vals[j];
+      T x = vals(j);
       for (int L = 0; L <= kMaxLevels; L++) {
         if (j & (1 << L)) {
           x = apply<OP>(x, stk[L]); /* op(upper block, lower block) */
@@ -251,9 +252,9 @@ __device__ T exact_value(const T *vals, int P, int p2s, int logp2s, int algo, bo
   const bool rab = algo != B200SHM_REC_DBL;
   for (int leaf = 0; leaf < p2s; leaf++) {
     const int as = p2s_member(leaf, P, p2s);
-    T x = vals[as];
+    T x = vals(as);
     if (p2s_extra(leaf, P, p2s)) {
-      const T ext = vals[as + 1];
+      const T ext = vals(as + 1);
       /* rec_dbl: op(extra, own) (reduce.c:241); Rabenseifner: op(extra,
        * own) on the lower half (397), op(own, extra) on the upper (375) */
       x = (!rab || lower_half) ? apply<OP>(ext, x) : apply<OP>(x, ext);
@@ -306,7 +307,8 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
     if (a.algo == B200SHM_REC_DBL) {
       /* every p2s member (and the extra folded into it) keeps its own value */
       for (int q = threadIdx.x; q < a.p2s; q += blockDim.x) {
-        const T v = exact_value<T, OP>(vals, a.P, a.p2s, a.logp2s, a.algo, lower, q);
+        const T v = exact_value<T, OP>([&](int j) { return vals[j]; }, a.P, a.p2s, a.logp2s,
+                                       a.algo, lower, q);
         const int as = p2s_member(q, a.P, a.p2s);
         memcpy(a.dst + (uint64_t)as * a.dstep + e * sizeof(T), &v, sizeof(T));
         if (p2s_extra(q, a.P, a.p2s))
@@ -317,7 +319,8 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
         int q = 0;
         if (a.algo != B200SHM_LINEAR && a.algo != B200SHM_BINOMIAL)
           q = rev_bits(rab_block(e, a.N, a.p2s), a.logp2s); /* owner of e's block */
-        common = exact_value<T, OP>(vals, a.P, a.p2s, a.logp2s, a.algo, lower, q);
+        common = exact_value<T, OP>([&](int j) { return vals[j]; }, a.P, a.p2s, a.logp2s, a.algo,
+                                    lower, q);
       }
       __syncthreads();
       for (int j = threadIdx.x; j < a.P; j += blockDim.x)
@@ -331,6 +334,9 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
 template <class T, int OP, int ORDER, int V, int U, bool MINMAX_CHECK, int LV>
 __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
   typedef Pack<T, V> PK;
+  /* grid-stride: all CTAs sweep one contiguous front of every member's
+   * slice together, which keeps DRAM row locality (contiguous per-CTA
+   * ranges measured ~20% slower) */
   const uint64_t gstride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.nvec; v += gstride) {
     const uint64_t e0 = a.e_begin + v * V;
@@ -361,43 +367,55 @@ __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
     } else {
       PK stk[LV]; /* LV levels hold trees of up to 2^LV - 1 leaves */
       const int nleaves = ORDER == ORD_BUTTERFLY ? a.p2s : a.P;
-      for (int q0 = 0; q0 < nleaves; q0 += U) {
-        PK x[U];
-        if constexpr (ORDER == ORD_BUTTERFLY) {
+      /* comb(lower block, upper block) in the algorithm's operand order */
+      auto comb = [](const PK &lo, const PK &hi) {
+        return ORDER == ORD_BUTTERFLY ? papply<OP>(lo, hi) : papply<OP>(hi, lo);
+      };
+      /* binary counter: pushing block number q at level `base` closes
+       * t = trailing_ones(q) blocks and parks the result at level base+t
+       * (all register indices static) */
+      auto push = [&](PK y, int q, int base) {
+        const int t = base + __ffs(~q) - 1;
 #pragma unroll
-          for (int u = 0; u < U; u++)
-            if (q0 + u < nleaves)
-              x[u] = ld_pack<T, V>(src + (uint64_t)p2s_member(q0 + u, a.P, a.p2s) * a.sstep);
-          if (a.P != a.p2s) {
-            /* fold the extra member into its p2s partner: op(extra, own) */
+        for (int L = 0; L < LV - 1; L++)
+          if (L >= base && L < t) y = comb(stk[L], y);
 #pragma unroll
-            for (int u = 0; u < U; u++)
-              if (q0 + u < nleaves && p2s_extra(q0 + u, a.P, a.p2s)) {
-                const int as = p2s_member(q0 + u, a.P, a.p2s);
-                x[u] = papply<OP>(ld_pack<T, V>(src + (uint64_t)(as + 1) * a.sstep), x[u]);
-              }
-          }
-        } else {
+        for (int L = 0; L < LV; L++)
+          if (L == t) stk[L] = y;
+      };
+      /* p2s member q is member ceil(q*P/p2s) (p2s is a power of two, so the
+       * division is a shift); it has an extra member folded into it exactly
+       * when the next p2s member is two members further on */
+      auto member_of = [&](int q) -> int {
+        return ORDER == ORD_BUTTERFLY
+                   ? (int)(((long long)q * a.P + a.p2s - 1) >> a.logp2s)
+                   : q;
+      };
+      auto leaf_addr = [&](int q) { return src + (uint64_t)member_of(q) * a.sstep; };
+      auto fold_extra = [&](PK &x, int q) {
+        /* rec_dbl / Rabenseifner fold the extra member in first as
+         * op(extra, own) (reduce.c:232-241) */
+        if (ORDER == ORD_BUTTERFLY && a.P != a.p2s && member_of(q + 1) - member_of(q) == 2)
+          x = papply<OP>(ld_pack<T, V>(leaf_addr(q) + a.sstep), x);
+      };
+      int q0 = 0;
+      /* full chunks of 8 leaves: 8 loads in flight, a fixed 8-leaf subtree */
+      for (; q0 + 8 <= nleaves; q0 += 8) {
+        PK x[8];
 #pragma unroll
-          for (int u = 0; u < U; u++)
-            if (q0 + u < nleaves) x[u] = ld_pack<T, V>(src + (uint64_t)(q0 + u) * a.sstep);
-        }
+        for (int u = 0; u < 8; u++) x[u] = ld_pack<T, V>(leaf_addr(q0 + u));
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          if (q0 + u < nleaves) {
-            /* binary counter: leaf q closes t = trailing_ones(q) blocks, then
-             * parks the merged block at level t (static register indices) */
-            const int q = q0 + u;
-            const int t = __ffs(~q) - 1;
-            PK y = x[u];
-#pragma unroll
-            for (int L = 0; L < LV - 1; L++)
-              if (L < t) y = ORDER == ORD_BUTTERFLY ? papply<OP>(stk[L], y) : papply<OP>(y, stk[L]);
-#pragma unroll
-            for (int L = 0; L < LV; L++)
-              if (L == t) stk[L] = y;
-          }
-        }
+        for (int u = 0; u < 8; u++) fold_extra(x[u], q0 + u);
+        const PK c = comb(comb(comb(x[0], x[1]), comb(x[2], x[3])),
+                          comb(comb(x[4], x[5]), comb(x[6], x[7])));
+        push(c, q0 >> 3, 3);
+      }
+      /* the last < 8 leaves (trees of < 8 leaves, binomial with P % 8 != 0) */
+#pragma unroll 1
+      for (; q0 < nleaves; q0++) {
+        PK x = ld_pack<T, V>(leaf_addr(q0));
+        fold_extra(x, q0);
+        push(x, q0, 0);
       }
       if constexpr (ORDER == ORD_BUTTERFLY) {
 #pragma unroll
@@ -434,25 +452,544 @@ __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
 
 /* Launch the packed body over [0, N - N%V) and a scalar tail, or scalar
  * throughout when the buffers are not 16-byte aligned. */
+/* ---- warp-cooperative variant ----------------------------------------
+ * G lanes (a power of two) share one 16-byte column.  Lane group g owns a
+ * contiguous share of the leaves -- for the butterfly and for binomial
+ * trees over a power-of-two team that share is a complete subtree -- and
+ * reduces it from loads it keeps 8 deep; the G partial results are then
+ * combined across lanes with __shfl_xor over masks 1, 2, ..., G/2, which
+ * is exactly the butterfly's remaining levels (mask m pairs group g with
+ * g^m, lower group first: reduce.c:250-272).  Every lane then stores the
+ * result to its own share of the members.  Registers per lane no longer
+ * grow with the tree depth, and a pack's 2*P memory operations are spread
+ * over G lanes. */
+template <class T, int V>
+__device__ __forceinline__ Pack<T, V> shfl_xor_pack(const Pack<T, V> &v, int m) {
+  static_assert(sizeof(Pack<T, V>) % 4 == 0, "pack of 32-bit words");
+  constexpr int W = (int)(sizeof(Pack<T, V>) / 4);
+  uint32_t w[W];
+  memcpy(w, &v, sizeof(w));
+#pragma unroll
+  for (int i = 0; i < W; i++) w[i] = __shfl_xor_sync(0xffffffffu, w[i], m);
+  Pack<T, V> r;
+  memcpy(&r, w, sizeof(w));
+  return r;
+}
+
+template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL>
+__global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
+  typedef Pack<T, V> PK;
+  constexpr int COLS = 32 / G; /* packs per warp per iteration */
+  const int lane = threadIdx.x & 31;
+  const int g = lane & (G - 1), c = lane / G;
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int P = a.P;
+  const int nleaves = ORDER == ORD_BUTTERFLY ? a.p2s : P;
+  /* this lane's leaves [l0, l1) */
+  const int l0 = (int)((long long)g * nleaves / G), l1 = (int)((long long)(g + 1) * nleaves / G);
+  /* members this lane stores to: [m0, m1) */
+  int m0, m1;
+  if (ORDER == ORD_BUTTERFLY) {
+    m0 = (int)(((long long)l0 * P + a.p2s - 1) >> a.logp2s);
+    m1 = (int)(((long long)l1 * P + a.p2s - 1) >> a.logp2s);
+  } else {
+    m0 = l0;
+    m1 = l1;
+  }
+  auto member_of = [&](int q) -> int {
+    return ORDER == ORD_BUTTERFLY ? (int)(((long long)q * P + a.p2s - 1) >> a.logp2s) : q;
+  };
+  auto comb = [](const PK &lo, const PK &hi) {
+    if constexpr (ORDER == ORD_BINOMIAL) return papply<OP>(hi, lo);
+    else return papply<OP>(lo, hi);
+  };
+  for (uint64_t base = warp * COLS; base < a.nvec; base += nwarps * COLS) {
+    const uint64_t v = base + c;
+    const bool live = v < a.nvec; /* uniform per column group */
+    const uint64_t e0 = a.e_begin + (live ? v : 0) * V;
+    const char *src = a.src + e0 * sizeof(T);
+    PK r;
+    unsigned cls[V];
+#pragma unroll
+    for (int i = 0; i < V; i++) cls[i] = 0;
+    if (live) {
+      if constexpr (ORDER == ORD_CHAIN) {
+        r = ld_pack<T, V>(src + (uint64_t)l0 * a.sstep);
+        if constexpr (MM) {
+#pragma unroll
+          for (int i = 0; i < V; i++) cls[i] = fclass(r.x[i]);
+        }
+        for (int j = l0 + 1; j < l1; j += 8) {
+          PK x[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j + u < l1) x[u] = ld_pack<T, V>(src + (uint64_t)(j + u) * a.sstep);
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j + u < l1) {
+              r = papply<OP>(r, x[u]);
+              if constexpr (MM) {
+#pragma unroll
+                for (int i = 0; i < V; i++) cls[i] |= fclass(x[u].x[i]);
+              }
+            }
+        }
+      } else {
+        /* complete subtree of l1-l0 (a power of two) leaves: chunks of 8
+         * as fixed subtrees, then a counter over the chunks (LVL levels
+         * hold up to 2^(LVL-1) chunks) */
+        PK stk[LVL];
+        const int n = l1 - l0;
+        auto leaf = [&](int q) {
+          PK x = ld_pack<T, V>(src + (uint64_t)member_of(q) * a.sstep);
+          return x;
+        };
+        auto fold = [&](PK &x, int q) {
+          if (ORDER == ORD_BUTTERFLY && P != a.p2s && member_of(q + 1) - member_of(q) == 2)
+            x = papply<OP>(ld_pack<T, V>(src + (uint64_t)(member_of(q) + 1) * a.sstep), x);
+        };
+        if (n >= 8) {
+          for (int q0 = 0; q0 < n; q0 += 8) {
+            PK x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = leaf(l0 + q0 + u);
+#pragma unroll
+            for (int u = 0; u < 8; u++) fold(x[u], l0 + q0 + u);
+            PK y = comb(comb(comb(x[0], x[1]), comb(x[2], x[3])),
+                        comb(comb(x[4], x[5]), comb(x[6], x[7])));
+            const int sidx = q0 >> 3, t = __ffs(~sidx) - 1;
+#pragma unroll
+            for (int L = 0; L < LVL - 1; L++)
+              if (L < t) y = comb(stk[L], y);
+#pragma unroll
+            for (int L = 0; L < LVL; L++)
+              if (L == t) stk[L] = y;
+          }
+          const int top = __ffs(n >> 3) - 1; /* log2(n/8) */
+#pragma unroll
+          for (int L = 0; L < LVL; L++)
+            if (L == top) r = stk[L];
+        } else {
+          PK x[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (u < n) {
+              x[u] = leaf(l0 + u);
+              fold(x[u], l0 + u);
+            }
+          r = n == 1 ? x[0] : n == 2 ? comb(x[0], x[1]) : comb(comb(x[0], x[1]), comb(x[2], x[3]));
+        }
+      }
+    }
+    /* butterfly levels across the G lanes of this column */
+#pragma unroll
+    for (int m = 1; m < G; m <<= 1) {
+      const PK o = shfl_xor_pack<T, V>(r, m);
+      r = (g & m) ? comb(o, r) : comb(r, o);
+      if constexpr (MM) {
+#pragma unroll
+        for (int i = 0; i < V; i++) cls[i] |= __shfl_xor_sync(0xffffffffu, cls[i], m);
+      }
+    }
+    if (!live) continue;
+    if constexpr (MM) {
+      bool amb = false;
+#pragma unroll
+      for (int i = 0; i < V; i++) amb |= ambiguous(cls[i]);
+      if (amb) { /* defer the pack; its dests stay untouched */
+        if (g == 0) {
+          const unsigned long long slot = atomicAdd(a.fix_count, (unsigned long long)V);
+          for (int i = 0; i < V; i++) {
+            if (slot + i < a.fix_cap) a.fix_list[slot + i] = e0 + i;
+            else atomicOr(a.status, (int)B200SHM_STATUS_FIX_OVERFLOW);
+          }
+        }
+        continue;
+      }
+    }
+    char *dst = a.dst + e0 * sizeof(T);
+    for (int j = m0; j < m1; j++) st_pack<T, V>(dst + (uint64_t)j * a.dstep, r);
+  }
+}
+
+/* ---- TMA-staged variant -------------------------------------------------
+ * The same reduction with the memory traffic done by the bulk-copy engine:
+ * per tile of TB bytes, one lane per member issues cp.async.bulk of that
+ * member's tile into a shared-memory stage (S stages deep, mbarrier
+ * completion); each thread combines one 16-byte column over the P staged
+ * rows; one lane per member bulk-stores the result tile back.  Bytes in
+ * flight no longer depend on registers.  Every mbarrier wait is bounded:
+ * on expiry the CTA sets the TIMEOUT status bit, drains what it issued
+ * (again bounded) and returns. */
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src, unsigned bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst_smem)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src_smem, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src_smem)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr long long kWaitSpins = 1ll << 26; /* ~seconds with nanosleep backoff */
+
+/* Bounded wait for phase `parity` of `bar`; false on expiry. */
+__device__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+  for (long long i = 0; i < kWaitSpins; i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (i > 64) __nanosleep(32);
+  }
+  return false;
+}
+
+struct TArgs {
+  RArgs r;
+  uint64_t ntiles;   /* full tiles of TB bytes per member */
+  unsigned TB;       /* tile bytes per member (multiple of 16)   */
+  int S;             /* pipeline stages                          */
+};
+
+template <class T, int OP, int ORDER, bool MM, int LV>
+__global__ void __launch_bounds__(128) k_reduce_tma(const TArgs ta) {
+  constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
+  typedef Pack<T, V> PK;
+  const RArgs &a = ta.r;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const unsigned TB = ta.TB;
+  const int S = ta.S, P = a.P;
+  const uint64_t stage_bytes = (uint64_t)P * TB;
+  uint64_t *bars = (uint64_t *)smem;                     /* S mbarriers       */
+  unsigned char *res = smem + 128;                       /* S result tiles    */
+  unsigned char *stages = res + (uint64_t)S * TB;        /* S x P x TB inputs */
+  const int tid = threadIdx.x;
+  const int packs = (int)(TB / 16);
+
+  if (tid == 0) {
+    for (int i = 0; i < S; i++) mbar_init(&bars[i], 1);
+    fence_async_smem();
+  }
+  __syncthreads();
+
+  /* tile k of this CTA is global tile blockIdx.x + k*gridDim.x */
+  const uint64_t my_tiles =
+      ta.ntiles > blockIdx.x ? (ta.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto issue = [&](uint64_t k) { /* warp 0: expect + one bulk copy per member */
+    const int s = (int)(k % S);
+    const uint64_t tile = blockIdx.x + k * gridDim.x;
+    const char *src = a.src + tile * TB;
+    unsigned char *dst = stages + (uint64_t)s * stage_bytes;
+    if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
+    __syncwarp();
+    for (int j = tid; j < P; j += 32) bulk_g2s(dst + (uint64_t)j * TB, src + (uint64_t)j * a.sstep, TB, &bars[s]);
+  };
+  if (tid < 32)
+    for (uint64_t k = 0; k < (uint64_t)(S - 1) && k < my_tiles; k++) issue(k);
+
+  bool dead = false;
+  for (uint64_t k = 0; k < my_tiles; k++) {
+    const int s = (int)(k % S);
+    /* refill the stage consumed in iteration k-1 (all threads are past it) */
+    if (tid < 32 && k + S - 1 < my_tiles) issue(k + S - 1);
+    if (!__syncthreads_and(mbar_wait_bounded(&bars[s], (unsigned)((k / S) & 1)))) {
+      if (tid == 0) atomicOr(a.status, (int)B200SHM_STATUS_TIMEOUT);
+      dead = true;
+      /* drain the loads issued for tiles k+1 .. k+S-2 (bounded) */
+      for (uint64_t d = k + 1; d < k + S - 1 && d < my_tiles; d++)
+        mbar_wait_bounded(&bars[d % S], (unsigned)((d / S) & 1));
+      break;
+    }
+    const unsigned char *in = stages + (uint64_t)s * stage_bytes;
+    const uint64_t tile = blockIdx.x + k * gridDim.x;
+    const uint64_t e0_tile = tile * (TB / sizeof(T));
+    bool amb = false;
+    if (tid < packs) {
+      auto row = [&](int j) { return *(const PK *)(in + (uint64_t)j * TB + tid * 16); };
+      PK r;
+      unsigned cls[V];
+      if constexpr (ORDER == ORD_CHAIN) {
+        r = row(0);
+        if constexpr (MM) {
+#pragma unroll
+          for (int i = 0; i < V; i++) cls[i] = fclass(r.x[i]);
+        }
+        for (int j = 1; j < P; j++) {
+          const PK x = row(j);
+          r = papply<OP>(r, x);
+          if constexpr (MM) {
+#pragma unroll
+            for (int i = 0; i < V; i++) cls[i] |= fclass(x.x[i]);
+          }
+        }
+      } else {
+        PK stk[LV];
+        const int nleaves = ORDER == ORD_BUTTERFLY ? a.p2s : P;
+        for (int q = 0; q < nleaves; q++) {
+          PK y;
+          if constexpr (ORDER == ORD_BUTTERFLY) {
+            const int as = (int)(((long long)q * P + a.p2s - 1) >> a.logp2s);
+            y = row(as);
+            if (P != a.p2s && (int)(((long long)(q + 1) * P + a.p2s - 1) >> a.logp2s) - as == 2)
+              y = papply<OP>(row(as + 1), y); /* op(extra, own) */
+          } else {
+            y = row(q);
+          }
+          const int t = __ffs(~q) - 1;
+#pragma unroll
+          for (int L = 0; L < LV - 1; L++)
+            if (L < t) y = ORDER == ORD_BUTTERFLY ? papply<OP>(stk[L], y) : papply<OP>(y, stk[L]);
+#pragma unroll
+          for (int L = 0; L < LV; L++)
+            if (L == t) stk[L] = y;
+        }
+        if constexpr (ORDER == ORD_BUTTERFLY) {
+#pragma unroll
+          for (int L = 0; L < LV; L++)
+            if (L == a.logp2s) r = stk[L];
+        } else {
+          bool have = false;
+#pragma unroll
+          for (int L = 0; L < LV; L++)
+            if (P & (1 << L)) {
+              r = have ? papply<OP>(r, stk[L]) : stk[L];
+              have = true;
+            }
+        }
+      }
+      if constexpr (MM) {
+#pragma unroll
+        for (int i = 0; i < V; i++) amb |= ambiguous(cls[i]);
+      }
+      /* the result tile of stage s was last bulk-stored S iterations ago;
+       * the issuing lane waited for that read before the barrier below */
+      *(PK *)(res + (uint64_t)s * TB + tid * 16) = r;
+    }
+    const bool tile_amb = MM ? __syncthreads_or(amb) : (__syncthreads(), false);
+    if (!tile_amb) {
+      fence_async_smem();
+      __syncthreads();
+      if (tid < 32) {
+        for (int j = tid; j < P; j += 32)
+          bulk_s2g(a.dst + (uint64_t)j * a.dstep + tile * TB, res + (uint64_t)s * TB, TB);
+        bulk_commit();
+      }
+    } else {
+      /* order-dependent MIN/MAX somewhere in this tile: replay the
+       * algorithm per element from the staged inputs and store per member
+       * (rec_dbl gives members different bits) */
+      const int E = (int)(TB / sizeof(T));
+      const int pairs = a.algo == B200SHM_REC_DBL ? a.p2s : 1;
+      for (int w = tid; w < E * pairs; w += blockDim.x) {
+        const int ei = w % E, q0 = w / E;
+        const uint64_t e = e0_tile + (uint64_t)ei;
+        auto get = [&](int j) { return *(const T *)(in + (uint64_t)j * TB + (uint64_t)ei * sizeof(T)); };
+        int q = q0;
+        if (a.algo == B200SHM_RABENSEIFNER || a.algo == B200SHM_RABENSEIFNER2)
+          q = rev_bits(rab_block(e, a.N, a.p2s), a.logp2s);
+        const T v = exact_value<T, OP>(get, P, a.p2s, a.logp2s, a.algo, e < a.N / 2, q);
+        if (a.algo == B200SHM_REC_DBL) {
+          const int as = p2s_member(q0, P, a.p2s);
+          memcpy(a.dst + (uint64_t)as * a.dstep + e * sizeof(T), &v, sizeof(T));
+          if (p2s_extra(q0, P, a.p2s))
+            memcpy(a.dst + (uint64_t)(as + 1) * a.dstep + e * sizeof(T), &v, sizeof(T));
+        } else {
+          for (int j = 0; j < P; j++) memcpy(a.dst + (uint64_t)j * a.dstep + e * sizeof(T), &v, sizeof(T));
+        }
+      }
+    }
+    /* before the next iteration refills stage (k+S)%S's sibling and, S
+     * iterations on, rewrites res[s]: all threads are done with this
+     * stage, and every store group but the newest has read its tile */
+    if (tid < 32) bulk_wait_read_1();
+    __syncthreads();
+  }
+  if (tid < 32) bulk_wait_all();
+  (void)dead;
+}
+
+/* Grid for one register-path launch: at most `occ` CTAs per SM (8 unless
+ * B200SHM_REDUCE_CTAS_PER_SM overrides it for tuning sweeps); CTAs
+ * grid-stride over the packs. */
+template <class K>
+unsigned reduce_grid(K kernel, int &occ, uint64_t nvec, int threads) {
+  (void)kernel;
+  if (occ < 0) { /* cached per kernel instantiation by the caller */
+    int o = 8; /* oversubscribed grid-stride grid: measured best */
+    const char *env = getenv("B200SHM_REDUCE_CTAS_PER_SM");
+    if (env && atoi(env) > 0) o = atoi(env);
+    occ = o;
+  }
+  const uint64_t need = (nvec + threads - 1) / threads;
+  const uint64_t cap = (uint64_t)st().sm_count * (uint64_t)occ;
+  return (unsigned)(need < cap ? (need ? need : 1) : cap);
+}
+
+/* Tile plan of the TMA path: the largest tile (and then the deepest
+ * pipeline) whose S x (P+1) x TB bytes fit one CTA's shared memory.
+ * B200SHM_REDUCE_PATH=regs disables it; B200SHM_TMA_TB / B200SHM_TMA_STAGES
+ * pin the plan (tuning sweeps). */
+struct TmaPlan {
+  unsigned TB = 0;
+  int S = 0;
+  size_t smem = 0;
+};
+constexpr size_t kMaxDynSmem = 227 * 1024;
+TmaPlan tma_plan(int P, uint64_t bytes_per_member) {
+  TmaPlan pl;
+  /* opt-in: on the 64-PE workload it measured below the register path
+   * (one 64-thread CTA per SM leaves the smem combine latency-bound) */
+  const char *path = getenv("B200SHM_REDUCE_PATH");
+  if (!path || strcmp(path, "tma") != 0) return pl;
+  const char *etb = getenv("B200SHM_TMA_TB"), *est = getenv("B200SHM_TMA_STAGES");
+  const unsigned tbs[] = {2048, 1024, 512};
+  for (unsigned tb : tbs) {
+    if (etb && (unsigned)atoi(etb) != tb) continue;
+    for (int S = 4; S >= 2; S--) {
+      if (est && atoi(est) != S) continue;
+      const size_t need = 128 + (size_t)S * tb * (size_t)(P + 1);
+      if (need <= kMaxDynSmem && bytes_per_member >= tb) {
+        pl.TB = tb;
+        pl.S = S;
+        pl.smem = need;
+        return pl;
+      }
+    }
+  }
+  return pl;
+}
+
 template <class T, int OP, int ORDER, bool MM, int LV>
 void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
   constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
   constexpr int U = ORDER == ORD_CHAIN ? 8 : 4;
+  static int occ_pack = -1, occ_tail = -1;
   RArgs a = base;
   uint64_t done = 0;
-  if (aligned && V > 1) {
-    a.e_begin = 0;
-    a.nvec = base.N / V;
-    if (a.nvec) {
-      k_reduce<T, OP, ORDER, V, U, MM, LV><<<grid_for(a.nvec, 256, 8), 256, 0, s>>>(a);
+  if (aligned) {
+    const TmaPlan pl = tma_plan(base.P, base.N * sizeof(T));
+    if (pl.TB) {
+      TArgs ta;
+      ta.r = base;
+      ta.TB = pl.TB;
+      ta.S = pl.S;
+      ta.ntiles = base.N * sizeof(T) / pl.TB;
+      auto k = k_reduce_tma<T, OP, ORDER, MM, LV>;
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+      const uint64_t per_sm = kMaxDynSmem / pl.smem;
+      uint64_t grid = (uint64_t)st().sm_count * (per_sm ? per_sm : 1);
+      if (grid > ta.ntiles) grid = ta.ntiles;
+      const int threads = pl.TB / 16 < 32 ? 32 : (int)(pl.TB / 16);
+      k<<<(unsigned)grid, threads, pl.smem, s>>>(ta);
       count_launch();
-      done = a.nvec * V;
+      done = ta.ntiles * (pl.TB / sizeof(T));
+    }
+  }
+  if (aligned && V > 1 && done < base.N) {
+    a.e_begin = done;
+    a.nvec = (base.N - done) / V;
+    if (a.nvec) {
+      /* warp-cooperative split of the leaves is exact for any-order ops,
+       * for butterflies, and for binomial trees over power-of-two teams.
+       * G lanes per column: 2 for chains, 4 for float trees (measured best
+       * on the 64-PE workload); B200SHM_REDUCE_COOP overrides (0 or 1 =
+       * one lane per column). */
+      constexpr bool any_order = ORDER == ORD_CHAIN && (std::is_integral<T>::value || MM);
+      const int nleaves = ORDER == ORD_BUTTERFLY ? base.p2s : base.P;
+      const bool splittable = any_order || ORDER == ORD_BUTTERFLY ||
+                              (ORDER == ORD_BINOMIAL && (base.P & (base.P - 1)) == 0);
+      int G = ORDER == ORD_CHAIN ? 2 : 4;
+      const char *ec = getenv("B200SHM_REDUCE_COOP");
+      if (ec) G = atoi(ec);
+      if (G < 1) G = 1;
+      if (G > 32) G = 32;
+      G = 1 << (31 - __builtin_clz((unsigned)G)); /* power of two */
+      while (G > 1 && G * 8 > nleaves) G >>= 1;
+      if constexpr (ORDER != ORD_CHAIN || any_order) {
+        if (splittable && G >= 2) {
+          const uint64_t lanes = a.nvec * (uint64_t)G;
+          const unsigned grid = grid_for(lanes, 256, 8);
+          const int chunks = nleaves / G / 8; /* tree chunks per lane */
+          if (ORDER == ORD_CHAIN || chunks <= 1) {
+            switch (G) {
+            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 1><<<grid, 256, 0, s>>>(a); break;
+            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 1><<<grid, 256, 0, s>>>(a); break;
+            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 1><<<grid, 256, 0, s>>>(a); break;
+            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 1><<<grid, 256, 0, s>>>(a); break;
+            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 1><<<grid, 256, 0, s>>>(a); break;
+            }
+          } else if (chunks <= 4) {
+            switch (G) {
+            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 3><<<grid, 256, 0, s>>>(a); break;
+            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 3><<<grid, 256, 0, s>>>(a); break;
+            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 3><<<grid, 256, 0, s>>>(a); break;
+            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 3><<<grid, 256, 0, s>>>(a); break;
+            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 3><<<grid, 256, 0, s>>>(a); break;
+            }
+          } else {
+            switch (G) {
+            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 7><<<grid, 256, 0, s>>>(a); break;
+            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 7><<<grid, 256, 0, s>>>(a); break;
+            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 7><<<grid, 256, 0, s>>>(a); break;
+            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 7><<<grid, 256, 0, s>>>(a); break;
+            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 7><<<grid, 256, 0, s>>>(a); break;
+            }
+          }
+          count_launch();
+          done += a.nvec * V;
+        }
+      }
+      if (done < base.N && a.e_begin == done) {
+        auto k = k_reduce<T, OP, ORDER, V, U, MM, LV>;
+        k<<<reduce_grid(k, occ_pack, a.nvec, 256), 256, 0, s>>>(a);
+        count_launch();
+        done += a.nvec * V;
+      }
     }
   }
   if (done < base.N) {
     a.e_begin = done;
     a.nvec = base.N - done;
-    k_reduce<T, OP, ORDER, 1, U, MM, LV><<<grid_for(a.nvec, 256, 8), 256, 0, s>>>(a);
+    auto k = k_reduce<T, OP, ORDER, 1, U, MM, LV>;
+    k<<<reduce_grid(k, occ_tail, a.nvec, 256), 256, 0, s>>>(a);
+    count_launch();
+  }
+  if constexpr (MM) {
+    k_minmax_fix<T, OP><<<2 * st().sm_count, 256, 0, s>>>(base, base.fix_list, base.fix_count,
+                                                         base.fix_cap);
     count_launch();
   }
 }
@@ -467,11 +1004,6 @@ int run(const RArgs &base, bool aligned, cudaStream_t s) {
       run_lv<T, OP, ORDER, MM, 8>(base, aligned, s);
     else
       run_lv<T, OP, ORDER, MM, kMaxLevels>(base, aligned, s);
-  }
-  if constexpr (MM) {
-    k_minmax_fix<T, OP><<<2 * st().sm_count, 256, 0, s>>>(base, base.fix_list, base.fix_count,
-                                                         base.fix_cap);
-    count_launch();
   }
   return B200SHM_OK;
 }
