@@ -208,6 +208,8 @@ def main():
                     help="time only dtype:op:algo (repeatable), e.g. float32:sum:rec_dbl")
     ap.add_argument("--heap-mb", type=int, default=HEAP >> 20, help="heap slice per PE (MiB)")
     ap.add_argument("--nelems", type=int, default=N, help="elements per PE")
+    ap.add_argument("--workload", default="reduce", choices=["reduce", "movement"],
+                    help="reduce (headline) or movement (alltoall/alltoalls/fcollect/AMO)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -221,6 +223,8 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.workload == "movement":
+        return run_movement(args, world, rank, local)
     dist = None
     if world > 1:
         import datetime
@@ -369,6 +373,79 @@ def main():
             "per_kernel_gbs": {k: round(v[1] / (v[0] / 1e3) / 1e9, 1) for k, v in durs.items()},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
     print(json.dumps(line), flush=True)
+
+# ---------------------------------------------------------------------------
+# data movement (the 128-PE configuration)
+# ---------------------------------------------------------------------------
+def run_movement(args, world, rank, local):
+    """128 emulated PEs: alltoallmem of 64 KiB per PE pair (uint8),
+    alltoalls64 with dst stride 2 / src stride 3 over 4096 int64 per pair,
+    fcollect64 of 4096 int64 per PE, and 2^20 int64 fetch-adds on 2^20
+    counters per PE at uniformly random (PE, offset).  Each op is timed on
+    its own with CUDA events over --steps launches."""
+    import torch
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    import gen
+    PM, BLK, NS, NF, NOPS, NCNT = 128, 64 << 10, 4096, 4096, 1 << 20, 1 << 20
+    B.init(PM, 96 << 20)  # 12 GiB arena: 76 MiB of objects per PE
+    team = (0, 1, PM)
+    s_ptr = B.stream()
+    st = torch.cuda.ExternalStream(s_ptr)
+    a2a_s, a2a_d = B.malloc(PM * BLK), B.malloc(PM * BLK)
+    B.put_rows(a2a_s, gen.uniform_int(np.uint8, PM, PM * BLK, 31), team=team)
+    as_s, as_d = B.malloc(PM * NS * 3 * 8), B.malloc(PM * NS * 2 * 8)
+    B.put_rows(as_s, gen.uniform_int(np.int64, PM, PM * NS * 3, 32), team=team)
+    fc_s, fc_d = B.malloc(NF * 8), B.malloc(PM * NF * 8)
+    B.put_rows(fc_s, gen.uniform_int(np.int64, PM, NF, 33), team=team)
+    cnt = B.malloc(NCNT * 8)
+    B.memset(cnt, 0, NCNT * 8, team=team)
+    rng = np.random.default_rng(34)
+    pe = rng.integers(0, PM, NOPS).astype(np.int32)
+    off = (cnt + rng.integers(0, NCNT, NOPS) * 8).astype(np.uint64)
+    req = B.malloc(NOPS * (4 + 8 + 8 + 8) + 4096)  # request arrays live in PE 0's slice
+    o_pe, o_off, o_val, o_f = req, req + NOPS * 4, req + NOPS * 12, req + NOPS * 20
+    for o, arr in ((o_pe, pe), (o_off, off), (o_val, np.ones(NOPS, np.int64))):
+        B.put_rows(o, arr.reshape(1, -1).view(np.uint8), team=(0, 1, 1))
+    d = {k: B.ptr(0, o) for k, o in (("pe", o_pe), ("off", o_off), ("val", o_val), ("f", o_f))}
+    ops = {
+        "alltoallmem": (lambda: B.alltoall(a2a_d, a2a_s, BLK, team=team, stream=s_ptr),
+                        2 * PM * PM * BLK, "GB/s"),
+        "alltoalls64": (lambda: B.alltoalls(as_d, as_s, 2, 3, NS, 8, team=team, stream=s_ptr),
+                        2 * PM * PM * NS * 8, "GB/s"),
+        "fcollect64": (lambda: B.fcollect(fc_d, fc_s, NF * 8, team=team, stream=s_ptr),
+                       PM * NF * 8 + PM * PM * NF * 8, "GB/s"),
+        "atomic_fetch_add": (lambda: B.amo_batch("fetch_add", "int64", NOPS, d["pe"], d["off"],
+                                                 d["val"], None, d["f"], stream=s_ptr),
+                             NOPS, "Mops/s"),
+    }
+    peak, peak_kind = peaks()
+    res = {}
+    launches0 = B.launch_count()
+    for name, (fn, units, unit) in ops.items():
+        for _ in range(args.warmup):
+            fn()
+        B.quiet()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn()
+        e1.record(st)
+        B.quiet()
+        ms = e0.elapsed_time(e1) / args.steps
+        rate = units / (ms / 1e3) / (1e9 if unit == "GB/s" else 1e6)
+        res[name] = {"ms": round(ms, 4), "value": round(rate, 1), "unit": unit}
+        if unit == "GB/s":
+            res[name]["frac_of_hbm"] = round(rate / peak, 4)
+    line = {"metric": METRIC, "workload": "movement", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "peak_gbs": peak, "peak_kind": peak_kind,
+            "config": {"npes": PM, "alltoallmem_block": BLK, "alltoalls": "int64 dst=2 sst=3 n=4096",
+                       "fcollect64_nelems": NF, "amo": "2^20 fetch_add int64 on 2^20 counters/PE"},
+            "results": res, "gpu_launches": B.launch_count() - launches0}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
 
 
 if __name__ == "__main__":

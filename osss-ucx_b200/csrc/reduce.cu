@@ -476,7 +476,7 @@ __device__ __forceinline__ Pack<T, V> shfl_xor_pack(const Pack<T, V> &v, int m) 
   return r;
 }
 
-template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL>
+template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL, bool POW2>
 __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
   typedef Pack<T, V> PK;
   constexpr int COLS = 32 / G; /* packs per warp per iteration */
@@ -537,27 +537,38 @@ __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
         }
       } else {
         /* complete subtree of l1-l0 (a power of two) leaves: chunks of 8
-         * as fixed subtrees, then a counter over the chunks (LVL levels
-         * hold up to 2^(LVL-1) chunks) */
-        PK stk[LVL];
+         * as fixed subtrees; LVL == 1: one chunk, LVL == 2: two chunks,
+         * else a counter over the chunks (LVL levels hold 2^(LVL-1)) */
         const int n = l1 - l0;
-        auto leaf = [&](int q) {
-          PK x = ld_pack<T, V>(src + (uint64_t)member_of(q) * a.sstep);
-          return x;
+        auto chunk = [&](int q0) {
+          PK x[8];
+          if constexpr (POW2) { /* member == leaf */
+            const char *p = src + (uint64_t)q0 * a.sstep;
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = ld_pack<T, V>(p + (uint64_t)u * a.sstep);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = ld_pack<T, V>(src + (uint64_t)member_of(q0 + u) * a.sstep);
+#pragma unroll
+            for (int u = 0; u < 8; u++) /* op(extra, own), reduce.c:232-241 */
+              if (member_of(q0 + u + 1) - member_of(q0 + u) == 2)
+                x[u] = papply<OP>(ld_pack<T, V>(src + (uint64_t)(member_of(q0 + u) + 1) * a.sstep), x[u]);
+          }
+          return comb(comb(comb(x[0], x[1]), comb(x[2], x[3])), comb(comb(x[4], x[5]), comb(x[6], x[7])));
         };
-        auto fold = [&](PK &x, int q) {
-          if (ORDER == ORD_BUTTERFLY && P != a.p2s && member_of(q + 1) - member_of(q) == 2)
-            x = papply<OP>(ld_pack<T, V>(src + (uint64_t)(member_of(q) + 1) * a.sstep), x);
-        };
-        if (n >= 8) {
+        if constexpr (LVL == 1) {
+          r = chunk(l0);
+        } else if constexpr (LVL == 2) {
+          /* two chunks, one at a time (keeps 8 loads in flight, not 16) */
+#pragma unroll 1
+          for (int c2 = 0; c2 < 2; c2++) {
+            const PK y = chunk(l0 + 8 * c2);
+            r = c2 ? comb(r, y) : y;
+          }
+        } else {
+          PK stk[LVL];
           for (int q0 = 0; q0 < n; q0 += 8) {
-            PK x[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) x[u] = leaf(l0 + q0 + u);
-#pragma unroll
-            for (int u = 0; u < 8; u++) fold(x[u], l0 + q0 + u);
-            PK y = comb(comb(comb(x[0], x[1]), comb(x[2], x[3])),
-                        comb(comb(x[4], x[5]), comb(x[6], x[7])));
+            PK y = chunk(l0 + q0);
             const int sidx = q0 >> 3, t = __ffs(~sidx) - 1;
 #pragma unroll
             for (int L = 0; L < LVL - 1; L++)
@@ -570,15 +581,6 @@ __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
 #pragma unroll
           for (int L = 0; L < LVL; L++)
             if (L == top) r = stk[L];
-        } else {
-          PK x[4];
-#pragma unroll
-          for (int u = 0; u < 4; u++)
-            if (u < n) {
-              x[u] = leaf(l0 + u);
-              fold(x[u], l0 + u);
-            }
-          r = n == 1 ? x[0] : n == 2 ? comb(x[0], x[1]) : comb(comb(x[0], x[1]), comb(x[2], x[3]));
         }
       }
     }
@@ -613,234 +615,6 @@ __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
   }
 }
 
-/* ---- TMA-staged variant -------------------------------------------------
- * The same reduction with the memory traffic done by the bulk-copy engine:
- * per tile of TB bytes, one lane per member issues cp.async.bulk of that
- * member's tile into a shared-memory stage (S stages deep, mbarrier
- * completion); each thread combines one 16-byte column over the P staged
- * rows; one lane per member bulk-stores the result tile back.  Bytes in
- * flight no longer depend on registers.  Every mbarrier wait is bounded:
- * on expiry the CTA sets the TIMEOUT status bit, drains what it issued
- * (again bounded) and returns. */
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src, unsigned bytes,
-                                         uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst_smem)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void bulk_s2g(void *dst, const void *src_smem, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-               "r"(smem_u32(src_smem)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_1() {
-  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-constexpr long long kWaitSpins = 1ll << 26; /* ~seconds with nanosleep backoff */
-
-/* Bounded wait for phase `parity` of `bar`; false on expiry. */
-__device__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
-  for (long long i = 0; i < kWaitSpins; i++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (i > 64) __nanosleep(32);
-  }
-  return false;
-}
-
-struct TArgs {
-  RArgs r;
-  uint64_t ntiles;   /* full tiles of TB bytes per member */
-  unsigned TB;       /* tile bytes per member (multiple of 16)   */
-  int S;             /* pipeline stages                          */
-};
-
-template <class T, int OP, int ORDER, bool MM, int LV>
-__global__ void __launch_bounds__(128) k_reduce_tma(const TArgs ta) {
-  constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
-  typedef Pack<T, V> PK;
-  const RArgs &a = ta.r;
-  extern __shared__ __align__(128) unsigned char smem[];
-  const unsigned TB = ta.TB;
-  const int S = ta.S, P = a.P;
-  const uint64_t stage_bytes = (uint64_t)P * TB;
-  uint64_t *bars = (uint64_t *)smem;                     /* S mbarriers       */
-  unsigned char *res = smem + 128;                       /* S result tiles    */
-  unsigned char *stages = res + (uint64_t)S * TB;        /* S x P x TB inputs */
-  const int tid = threadIdx.x;
-  const int packs = (int)(TB / 16);
-
-  if (tid == 0) {
-    for (int i = 0; i < S; i++) mbar_init(&bars[i], 1);
-    fence_async_smem();
-  }
-  __syncthreads();
-
-  /* tile k of this CTA is global tile blockIdx.x + k*gridDim.x */
-  const uint64_t my_tiles =
-      ta.ntiles > blockIdx.x ? (ta.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  auto issue = [&](uint64_t k) { /* warp 0: expect + one bulk copy per member */
-    const int s = (int)(k % S);
-    const uint64_t tile = blockIdx.x + k * gridDim.x;
-    const char *src = a.src + tile * TB;
-    unsigned char *dst = stages + (uint64_t)s * stage_bytes;
-    if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
-    __syncwarp();
-    for (int j = tid; j < P; j += 32) bulk_g2s(dst + (uint64_t)j * TB, src + (uint64_t)j * a.sstep, TB, &bars[s]);
-  };
-  if (tid < 32)
-    for (uint64_t k = 0; k < (uint64_t)(S - 1) && k < my_tiles; k++) issue(k);
-
-  bool dead = false;
-  for (uint64_t k = 0; k < my_tiles; k++) {
-    const int s = (int)(k % S);
-    /* refill the stage consumed in iteration k-1 (all threads are past it) */
-    if (tid < 32 && k + S - 1 < my_tiles) issue(k + S - 1);
-    if (!__syncthreads_and(mbar_wait_bounded(&bars[s], (unsigned)((k / S) & 1)))) {
-      if (tid == 0) atomicOr(a.status, (int)B200SHM_STATUS_TIMEOUT);
-      dead = true;
-      /* drain the loads issued for tiles k+1 .. k+S-2 (bounded) */
-      for (uint64_t d = k + 1; d < k + S - 1 && d < my_tiles; d++)
-        mbar_wait_bounded(&bars[d % S], (unsigned)((d / S) & 1));
-      break;
-    }
-    const unsigned char *in = stages + (uint64_t)s * stage_bytes;
-    const uint64_t tile = blockIdx.x + k * gridDim.x;
-    const uint64_t e0_tile = tile * (TB / sizeof(T));
-    bool amb = false;
-    if (tid < packs) {
-      auto row = [&](int j) { return *(const PK *)(in + (uint64_t)j * TB + tid * 16); };
-      PK r;
-      unsigned cls[V];
-      if constexpr (ORDER == ORD_CHAIN) {
-        r = row(0);
-        if constexpr (MM) {
-#pragma unroll
-          for (int i = 0; i < V; i++) cls[i] = fclass(r.x[i]);
-        }
-        for (int j = 1; j < P; j++) {
-          const PK x = row(j);
-          r = papply<OP>(r, x);
-          if constexpr (MM) {
-#pragma unroll
-            for (int i = 0; i < V; i++) cls[i] |= fclass(x.x[i]);
-          }
-        }
-      } else {
-        PK stk[LV];
-        const int nleaves = ORDER == ORD_BUTTERFLY ? a.p2s : P;
-        for (int q = 0; q < nleaves; q++) {
-          PK y;
-          if constexpr (ORDER == ORD_BUTTERFLY) {
-            const int as = (int)(((long long)q * P + a.p2s - 1) >> a.logp2s);
-            y = row(as);
-            if (P != a.p2s && (int)(((long long)(q + 1) * P + a.p2s - 1) >> a.logp2s) - as == 2)
-              y = papply<OP>(row(as + 1), y); /* op(extra, own) */
-          } else {
-            y = row(q);
-          }
-          const int t = __ffs(~q) - 1;
-#pragma unroll
-          for (int L = 0; L < LV - 1; L++)
-            if (L < t) y = ORDER == ORD_BUTTERFLY ? papply<OP>(stk[L], y) : papply<OP>(y, stk[L]);
-#pragma unroll
-          for (int L = 0; L < LV; L++)
-            if (L == t) stk[L] = y;
-        }
-        if constexpr (ORDER == ORD_BUTTERFLY) {
-#pragma unroll
-          for (int L = 0; L < LV; L++)
-            if (L == a.logp2s) r = stk[L];
-        } else {
-          bool have = false;
-#pragma unroll
-          for (int L = 0; L < LV; L++)
-            if (P & (1 << L)) {
-              r = have ? papply<OP>(r, stk[L]) : stk[L];
-              have = true;
-            }
-        }
-      }
-      if constexpr (MM) {
-#pragma unroll
-        for (int i = 0; i < V; i++) amb |= ambiguous(cls[i]);
-      }
-      /* the result tile of stage s was last bulk-stored S iterations ago;
-       * the issuing lane waited for that read before the barrier below */
-      *(PK *)(res + (uint64_t)s * TB + tid * 16) = r;
-    }
-    const bool tile_amb = MM ? __syncthreads_or(amb) : (__syncthreads(), false);
-    if (!tile_amb) {
-      fence_async_smem();
-      __syncthreads();
-      if (tid < 32) {
-        for (int j = tid; j < P; j += 32)
-          bulk_s2g(a.dst + (uint64_t)j * a.dstep + tile * TB, res + (uint64_t)s * TB, TB);
-        bulk_commit();
-      }
-    } else {
-      /* order-dependent MIN/MAX somewhere in this tile: replay the
-       * algorithm per element from the staged inputs and store per member
-       * (rec_dbl gives members different bits) */
-      const int E = (int)(TB / sizeof(T));
-      const int pairs = a.algo == B200SHM_REC_DBL ? a.p2s : 1;
-      for (int w = tid; w < E * pairs; w += blockDim.x) {
-        const int ei = w % E, q0 = w / E;
-        const uint64_t e = e0_tile + (uint64_t)ei;
-        auto get = [&](int j) { return *(const T *)(in + (uint64_t)j * TB + (uint64_t)ei * sizeof(T)); };
-        int q = q0;
-        if (a.algo == B200SHM_RABENSEIFNER || a.algo == B200SHM_RABENSEIFNER2)
-          q = rev_bits(rab_block(e, a.N, a.p2s), a.logp2s);
-        const T v = exact_value<T, OP>(get, P, a.p2s, a.logp2s, a.algo, e < a.N / 2, q);
-        if (a.algo == B200SHM_REC_DBL) {
-          const int as = p2s_member(q0, P, a.p2s);
-          memcpy(a.dst + (uint64_t)as * a.dstep + e * sizeof(T), &v, sizeof(T));
-          if (p2s_extra(q0, P, a.p2s))
-            memcpy(a.dst + (uint64_t)(as + 1) * a.dstep + e * sizeof(T), &v, sizeof(T));
-        } else {
-          for (int j = 0; j < P; j++) memcpy(a.dst + (uint64_t)j * a.dstep + e * sizeof(T), &v, sizeof(T));
-        }
-      }
-    }
-    /* before the next iteration refills stage (k+S)%S's sibling and, S
-     * iterations on, rewrites res[s]: all threads are done with this
-     * stage, and every store group but the newest has read its tile */
-    if (tid < 32) bulk_wait_read_1();
-    __syncthreads();
-  }
-  if (tid < 32) bulk_wait_all();
-  (void)dead;
-}
-
 /* Grid for one register-path launch: at most `occ` CTAs per SM (8 unless
  * B200SHM_REDUCE_CTAS_PER_SM overrides it for tuning sweeps); CTAs
  * grid-stride over the packs. */
@@ -858,38 +632,34 @@ unsigned reduce_grid(K kernel, int &occ, uint64_t nvec, int threads) {
   return (unsigned)(need < cap ? (need ? need : 1) : cap);
 }
 
-/* Tile plan of the TMA path: the largest tile (and then the deepest
- * pipeline) whose S x (P+1) x TB bytes fit one CTA's shared memory.
- * B200SHM_REDUCE_PATH=regs disables it; B200SHM_TMA_TB / B200SHM_TMA_STAGES
- * pin the plan (tuning sweeps). */
-struct TmaPlan {
-  unsigned TB = 0;
-  int S = 0;
-  size_t smem = 0;
-};
-constexpr size_t kMaxDynSmem = 227 * 1024;
-TmaPlan tma_plan(int P, uint64_t bytes_per_member) {
-  TmaPlan pl;
-  /* opt-in: on the 64-PE workload it measured below the register path
-   * (one 64-thread CTA per SM leaves the smem combine latency-bound) */
-  const char *path = getenv("B200SHM_REDUCE_PATH");
-  if (!path || strcmp(path, "tma") != 0) return pl;
-  const char *etb = getenv("B200SHM_TMA_TB"), *est = getenv("B200SHM_TMA_STAGES");
-  const unsigned tbs[] = {2048, 1024, 512};
-  for (unsigned tb : tbs) {
-    if (etb && (unsigned)atoi(etb) != tb) continue;
-    for (int S = 4; S >= 2; S--) {
-      if (est && atoi(est) != S) continue;
-      const size_t need = 128 + (size_t)S * tb * (size_t)(P + 1);
-      if (need <= kMaxDynSmem && bytes_per_member >= tb) {
-        pl.TB = tb;
-        pl.S = S;
-        pl.smem = need;
-        return pl;
-      }
+template <class T, int OP, int ORDER, int V, bool MM, int G>
+void launch_coop_g(int lvl, bool pow2, unsigned grid, cudaStream_t s, const RArgs &a) {
+  if constexpr (ORDER == ORD_CHAIN) {
+    k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
+  } else if constexpr (ORDER == ORD_BINOMIAL) { /* only power-of-two teams get here */
+    if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
+    else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true><<<grid, 256, 0, s>>>(a);
+    else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true><<<grid, 256, 0, s>>>(a);
+  } else {
+    if (pow2) {
+      if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
+      else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true><<<grid, 256, 0, s>>>(a);
+      else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true><<<grid, 256, 0, s>>>(a);
+    } else {
+      if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, false><<<grid, 256, 0, s>>>(a);
+      else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, false><<<grid, 256, 0, s>>>(a);
+      else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, false><<<grid, 256, 0, s>>>(a);
     }
   }
-  return pl;
+}
+
+template <class T, int OP, int ORDER, int V, bool MM>
+void launch_coop(int G, int lvl, bool pow2, unsigned grid, cudaStream_t s, const RArgs &a) {
+  switch (G) {
+  case 2: launch_coop_g<T, OP, ORDER, V, MM, 2>(lvl, pow2, grid, s, a); break;
+  case 4: launch_coop_g<T, OP, ORDER, V, MM, 4>(lvl, pow2, grid, s, a); break;
+  default: launch_coop_g<T, OP, ORDER, V, MM, 8>(lvl, pow2, grid, s, a); break;
+  }
 }
 
 template <class T, int OP, int ORDER, bool MM, int LV>
@@ -899,25 +669,6 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
   static int occ_pack = -1, occ_tail = -1;
   RArgs a = base;
   uint64_t done = 0;
-  if (aligned) {
-    const TmaPlan pl = tma_plan(base.P, base.N * sizeof(T));
-    if (pl.TB) {
-      TArgs ta;
-      ta.r = base;
-      ta.TB = pl.TB;
-      ta.S = pl.S;
-      ta.ntiles = base.N * sizeof(T) / pl.TB;
-      auto k = k_reduce_tma<T, OP, ORDER, MM, LV>;
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
-      const uint64_t per_sm = kMaxDynSmem / pl.smem;
-      uint64_t grid = (uint64_t)st().sm_count * (per_sm ? per_sm : 1);
-      if (grid > ta.ntiles) grid = ta.ntiles;
-      const int threads = pl.TB / 16 < 32 ? 32 : (int)(pl.TB / 16);
-      k<<<(unsigned)grid, threads, pl.smem, s>>>(ta);
-      count_launch();
-      done = ta.ntiles * (pl.TB / sizeof(T));
-    }
-  }
   if (aligned && V > 1 && done < base.N) {
     a.e_begin = done;
     a.nvec = (base.N - done) / V;
@@ -936,6 +687,7 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
       if (ec) G = atoi(ec);
       if (G < 1) G = 1;
       if (G > 32) G = 32;
+      if (G > 8) G = 8;
       G = 1 << (31 - __builtin_clz((unsigned)G)); /* power of two */
       while (G > 1 && G * 8 > nleaves) G >>= 1;
       if constexpr (ORDER != ORD_CHAIN || any_order) {
@@ -943,31 +695,9 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
           const uint64_t lanes = a.nvec * (uint64_t)G;
           const unsigned grid = grid_for(lanes, 256, 8);
           const int chunks = nleaves / G / 8; /* tree chunks per lane */
-          if (ORDER == ORD_CHAIN || chunks <= 1) {
-            switch (G) {
-            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 1><<<grid, 256, 0, s>>>(a); break;
-            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 1><<<grid, 256, 0, s>>>(a); break;
-            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 1><<<grid, 256, 0, s>>>(a); break;
-            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 1><<<grid, 256, 0, s>>>(a); break;
-            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 1><<<grid, 256, 0, s>>>(a); break;
-            }
-          } else if (chunks <= 4) {
-            switch (G) {
-            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 3><<<grid, 256, 0, s>>>(a); break;
-            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 3><<<grid, 256, 0, s>>>(a); break;
-            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 3><<<grid, 256, 0, s>>>(a); break;
-            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 3><<<grid, 256, 0, s>>>(a); break;
-            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 3><<<grid, 256, 0, s>>>(a); break;
-            }
-          } else {
-            switch (G) {
-            case 2: k_reduce_coop<T, OP, ORDER, V, 2, MM, 7><<<grid, 256, 0, s>>>(a); break;
-            case 4: k_reduce_coop<T, OP, ORDER, V, 4, MM, 7><<<grid, 256, 0, s>>>(a); break;
-            case 8: k_reduce_coop<T, OP, ORDER, V, 8, MM, 7><<<grid, 256, 0, s>>>(a); break;
-            case 16: k_reduce_coop<T, OP, ORDER, V, 16, MM, 7><<<grid, 256, 0, s>>>(a); break;
-            default: k_reduce_coop<T, OP, ORDER, V, 32, MM, 7><<<grid, 256, 0, s>>>(a); break;
-            }
-          }
+          const bool pow2 = ORDER != ORD_BUTTERFLY || base.P == base.p2s;
+          launch_coop<T, OP, ORDER, V, MM>(G, ORDER == ORD_CHAIN ? 1 : chunks <= 1 ? 1 : chunks == 2 ? 2 : 7,
+                                           pow2, grid, s, a);
           count_launch();
           done += a.nvec * V;
         }
