@@ -781,10 +781,10 @@ int run_int(int op, const RArgs &a, bool aligned, cudaStream_t s) {
 static const int kDtypeSize[B200SHM_NDTYPE] = {1, 2, 4, 8, 1, 2, 4, 8, 4, 8, 16, 8, 16};
 
 /* Host side of b200shm_reduce, also used by the batched and serving paths. */
-int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
-                  uint64_t dest_off, uint64_t src_off, uint64_t nelems, cudaStream_t s) {
-  int rc = check_team(pe_start, pe_stride, pe_size);
-  if (rc) return rc;
+/* Checks shared by every reduce entry point: the (op, dtype, algo) triple
+ * exists in the reference's type tables, and the team size fits the
+ * combine trees of the GPU kernels. */
+static int reduce_check(int op, int dtype, int algo, int pe_size) {
   if (op < 0 || op >= B200SHM_NOP || dtype < 0 || dtype >= B200SHM_NDTYPE || algo < 0 ||
       algo >= B200SHM_NALGO)
     return fail(B200SHM_ERR_ARG, "reduce: bad op %d / dtype %d / algo %d", op, dtype, algo);
@@ -795,19 +795,9 @@ int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int 
   if (dtype == B200SHM_F80)
     return fail(B200SHM_ERR_UNSUPPORTED,
                 "reduce: long double (x87 80-bit) arithmetic is not available on the GPU");
-  const uint64_t es = (uint64_t)kDtypeSize[dtype];
-  if (nelems > st().slice / es) return fail(B200SHM_ERR_ARG, "reduce: nelems too large");
-  const uint64_t bytes = nelems * es;
-  if ((rc = check_extent(src_off, bytes, "reduce source"))) return rc;
-  if ((rc = check_extent(dest_off, bytes, "reduce dest"))) return rc;
-  if (dest_off != src_off && overlaps(dest_off, bytes, src_off, bytes))
-    return fail(B200SHM_ERR_ARG, "reduce: dest and source overlap without being identical");
-  if (nelems == 0) return B200SHM_OK;
-  int logp = 0, p2s = 1;
-  while (p2s * 2 <= pe_size) {
-    p2s *= 2;
-    logp++;
-  }
+  if (pe_size < 1) return fail(B200SHM_ERR_ARG, "reduce: team size %d < 1", pe_size);
+  int p2s = 1;
+  while (p2s * 2 <= pe_size) p2s *= 2;
   const bool tree = !is_int && op != B200SHM_MIN && op != B200SHM_MAX && algo != B200SHM_LINEAR;
   const int leaves = algo == B200SHM_BINOMIAL ? pe_size : p2s;
   if (tree && leaves > (1 << (kMaxLevels - 1)))
@@ -816,23 +806,58 @@ int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int 
   if (!is_int && (op == B200SHM_MIN || op == B200SHM_MAX) && pe_size > kFixMaxMembers)
     return fail(B200SHM_ERR_UNSUPPORTED, "reduce: float MIN/MAX is limited to %d members",
                 kFixMaxMembers);
-  Members m = members(pe_start, pe_stride, pe_size);
+  return B200SHM_OK;
+}
+
+static RArgs reduce_args(const char *src, char *dst, uint64_t sstep, uint64_t dstep, int P,
+                         uint64_t nelems, int algo) {
   RArgs a;
-  a.src = m.first + src_off;
-  a.dst = m.first + dest_off;
-  a.sstep = a.dstep = m.step;
+  int logp = 0, p2s = 1;
+  while (p2s * 2 <= P) {
+    p2s *= 2;
+    logp++;
+  }
+  a.src = src;
+  a.dst = dst;
+  a.sstep = sstep;
+  a.dstep = dstep;
   a.e_begin = 0;
   a.nvec = 0;
   a.N = nelems;
-  a.P = pe_size;
+  a.P = P;
   a.p2s = p2s;
   a.logp2s = logp;
   a.algo = algo;
+  return a;
+}
+
+static int reduce_dispatch(int op, int dtype, const RArgs &a, bool aligned, cudaStream_t s);
+
+int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
+                  uint64_t dest_off, uint64_t src_off, uint64_t nelems, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, pe_size);
+  if (rc) return rc;
+  if ((rc = reduce_check(op, dtype, algo, pe_size))) return rc;
+  const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  if (nelems > st().slice / es) return fail(B200SHM_ERR_ARG, "reduce: nelems too large");
+  const uint64_t bytes = nelems * es;
+  if ((rc = check_extent(src_off, bytes, "reduce source"))) return rc;
+  if ((rc = check_extent(dest_off, bytes, "reduce dest"))) return rc;
+  if (dest_off != src_off && overlaps(dest_off, bytes, src_off, bytes))
+    return fail(B200SHM_ERR_ARG, "reduce: dest and source overlap without being identical");
+  if (nelems == 0) return B200SHM_OK;
+  Members m = members(pe_start, pe_stride, pe_size);
+  RArgs a = reduce_args(m.first + src_off, m.first + dest_off, m.step, m.step, pe_size, nelems,
+                        algo);
   a.fix_list = st().fix_list;
   a.fix_count = st().fix_count;
   a.fix_cap = st().fix_cap;
   a.status = st().d_status;
   const bool aligned = ((src_off | dest_off | m.step) & 15u) == 0;
+  return reduce_dispatch(op, dtype, a, aligned, s);
+}
+
+static int reduce_dispatch(int op, int dtype, const RArgs &a, bool aligned, cudaStream_t s) {
   switch (dtype) {
   case B200SHM_I8: return run_int<int8_t, uint8_t>(op, a, aligned, s);
   case B200SHM_I16: return run_int<int16_t, uint16_t>(op, a, aligned, s);
