@@ -98,6 +98,23 @@ int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_stride,
                    int pe_size, uint64_t dest_off, uint64_t src_off,
                    uint64_t nelems, void *stream);
 
+/* The same all-reduce for callers that cannot allocate device memory (a
+ * runtime that owns every device allocation through its own pool, or code
+ * that may not call cudaMalloc at all).  No counterpart in the reference.
+ * It needs no b200shm_init and allocates nothing: member i's rows are the
+ * caller's device buffers source + i*source_stride and dest + i*dest_stride.
+ * Float MIN/MAX keeps its list of order-dependent elements in a file-scope
+ * static device array (2 MiB + 256 bytes per GPU that loads the library,
+ * held until exit), so float MIN/MAX is limited to 2^18 elements per
+ * member; larger sizes are rejected with B200SHM_ERR_UNSUPPORTED.  All
+ * calls share that array: calls that overlap on the GPU race.  The first
+ * call on a device resolves the array's device address (set-up), so make
+ * it before any stream capture.  The call blocks until the result is in
+ * every dest (on `stream`, or the default stream when NULL). */
+int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, void *dest,
+                           uint64_t dest_stride, const void *source,
+                           uint64_t source_stride, uint64_t nelems, void *stream);
+
 /* Fixed-size allgather: member j's dest[k*nbytes ..] = member k's source.
  * Replaces fcollect_helper_* (src/shcoll/src/fcollect.c:32-484) behind
  * shcoll_fcollect{32,64}_<algo>, shcoll_<T>_fcollect_<algo> and

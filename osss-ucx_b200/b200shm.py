@@ -61,6 +61,7 @@ def _load():
         "b200shm_get_host": (ci, [vp, ci, ci, ci, u64, u64, vp]),
         "b200shm_memset": (ci, [ci, ci, ci, u64, ci, u64, vp]),
         "b200shm_reduce": (ci, [ci, ci, ci, ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_reduce_noalloc": (ci, [ci, ci, ci, ci, vp, u64, vp, u64, u64, vp]),
         "b200shm_fcollect": (ci, [ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_alltoall": (ci, [ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_alltoalls": (ci, [ci, ci, ci, u64, u64, i64, i64, u64, u64, vp]),
@@ -162,6 +163,15 @@ def reduce(op, dtype, algo, dest, src, nelems, team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_reduce(OPS.index(op), DTYPES.index(dtype), ALGOS.index(algo),
                                      start, stride, size, dest, src, nelems, stream))
+
+
+def reduce_noalloc(op, dtype, algo, npes, dest_ptr, dest_stride, src_ptr, src_stride, nelems,
+                   stream=None):
+    """All-reduce over caller-owned device buffers (device addresses as ints);
+    allocates nothing and needs no init()."""
+    return _check(lib.b200shm_reduce_noalloc(OPS.index(op), DTYPES.index(dtype),
+                                             ALGOS.index(algo), npes, dest_ptr, dest_stride,
+                                             src_ptr, src_stride, nelems, stream))
 
 
 def fcollect(dest, src, nbytes, team=None, stream=None):

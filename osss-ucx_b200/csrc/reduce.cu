@@ -34,6 +34,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <type_traits>
 
 #include "internal.cuh"
@@ -899,4 +900,105 @@ extern "C" int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_
                                nelems, b200::pick_stream(stream));
   if (rc) return rc;
   return b200::finish(stream, "b200shm_reduce");
+}
+
+/* ---------------------------------------------------------------------------
+ * b200shm_reduce_noalloc: the all-reduce for callers that cannot allocate
+ * device memory.
+ *
+ * Some callers of this code cannot call cudaMalloc: a host runtime that
+ * owns all device memory through its own pool, code running inside a
+ * captured or otherwise allocation-restricted region, or an embedding that
+ * hands the engine pre-registered buffers and forbids it any allocation of
+ * its own.  They cannot use b200shm_reduce either, because that needs the
+ * arena and the deferred-element list that b200shm_init allocates.  This
+ * entry point takes caller-owned device buffers directly and allocates
+ * nothing: the one piece of scratch the reduction needs -- the list of
+ * float MIN/MAX elements whose result depends on operand order (NaN, or
+ * both +0 and -0, among the inputs), plus its counter and a status word --
+ * lives in the file-scope array below, which every GPU that loads this
+ * library holds until the process exits.
+ * ------------------------------------------------------------------------- */
+namespace b200 {
+
+/* at most this many elements per member for a float MIN/MAX reduction,
+ * since in the worst case every element is deferred */
+constexpr uint64_t kNoAllocMaxDeferred = 1ull << 18;
+/* [0] deferred count, [1] status bits, [32 ..] deferred element indices:
+ * 2 MiB + 256 bytes */
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[32 + kNoAllocMaxDeferred];
+
+/* Device address of g_noalloc_scratch, resolved once per device with that
+ * device current (in host code the symbol names a host-side stand-in). */
+static int noalloc_scratch(unsigned long long **out) {
+  static std::mutex mu;
+  static unsigned long long *addr[256] = {nullptr};
+  int dev = 0;
+  B200_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(B200SHM_ERR_UNSUPPORTED, "device ordinal %d", dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (addr[dev] == nullptr) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    addr[dev] = (unsigned long long *)p;
+  }
+  *out = addr[dev];
+  return B200SHM_OK;
+}
+
+}  // namespace b200
+
+extern "C" int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, void *dest,
+                                      uint64_t dest_stride, const void *source,
+                                      uint64_t source_stride, uint64_t nelems, void *stream) {
+  using namespace b200;
+  int rc = reduce_check(op, dtype, algo, npes);
+  if (rc) return rc;
+  if (nelems == 0) return B200SHM_OK;
+  if (dest == nullptr || source == nullptr)
+    return fail(B200SHM_ERR_ARG, "reduce_noalloc: null buffer");
+  const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  const uint64_t bytes = nelems * es;
+  if (npes > 1 && (dest_stride < bytes || source_stride < bytes))
+    return fail(B200SHM_ERR_ARG, "reduce_noalloc: member stride smaller than the %llu-byte row",
+                (unsigned long long)bytes);
+  if (dest != source) {
+    /* a member's dest row must not overlap its source row unless the two
+     * are the same buffer (in place), as for b200shm_reduce */
+    const char *d0 = (const char *)dest, *s0 = (const char *)source;
+    if (dest_stride == source_stride && d0 < s0 + bytes && s0 < d0 + bytes)
+      return fail(B200SHM_ERR_ARG, "reduce_noalloc: dest and source overlap without being identical");
+  }
+  const bool minmax_float = (op == B200SHM_MIN || op == B200SHM_MAX) &&
+                            (dtype == B200SHM_F32 || dtype == B200SHM_F64);
+  if (minmax_float && nelems > kNoAllocMaxDeferred)
+    return fail(B200SHM_ERR_UNSUPPORTED,
+                "reduce_noalloc: float MIN/MAX is limited to %llu elements per member (the "
+                "static deferred list); use b200shm_reduce for more",
+                (unsigned long long)kNoAllocMaxDeferred);
+  unsigned long long *scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  RArgs a = reduce_args((const char *)source, (char *)dest, source_stride, dest_stride, npes,
+                        nelems, algo);
+  a.fix_count = scratch;
+  a.status = (int *)(scratch + 1);
+  a.fix_list = scratch + 32;
+  a.fix_cap = kNoAllocMaxDeferred;
+  /* the scratch keeps the previous call's contents: clear the counter and
+   * the status word first */
+  B200_CK(cudaMemsetAsync(scratch, 0, 2 * sizeof(unsigned long long), s));
+  const bool aligned = (((uintptr_t)dest | (uintptr_t)source | dest_stride | source_stride) & 15u) == 0;
+  if ((rc = reduce_dispatch(op, dtype, a, aligned, s))) return rc;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "b200shm_reduce_noalloc launch");
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "b200shm_reduce_noalloc");
+  unsigned long long status = 0;
+  e = cudaMemcpy(&status, scratch + 1, sizeof(status), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "b200shm_reduce_noalloc status");
+  if (status)
+    return fail(B200SHM_ERR_NOMEM, "reduce_noalloc: deferred-element list overflowed");
+  return B200SHM_OK;
 }
