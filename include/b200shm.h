@@ -79,6 +79,10 @@ int b200shm_put_host(int pe_start, int pe_stride, int pe_count, uint64_t off,
                      const void *host_src, uint64_t bytes_per_pe, void *stream);
 int b200shm_get_host(void *host_dst, int pe_start, int pe_stride, int pe_count,
                      uint64_t off, uint64_t bytes_per_pe, void *stream);
+/* Copy between any two addresses the device can see (heap, device, managed
+ * or host memory); blocking when stream is NULL.  Backs shmem_putmem /
+ * shmem_getmem (src/shmemc/ucx/comms.c:677-737). */
+int b200shm_memcpy(void *dst, const void *src, uint64_t bytes, void *stream);
 /* Fill bytes_per_pe bytes at `off` of pe_count members with `byte`. */
 int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off,
                    int byte, uint64_t bytes_per_pe, void *stream);
@@ -173,6 +177,15 @@ int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size,
 int b200shm_amo_batch(int amo, int dtype, uint64_t nops, const int32_t *pe,
                       const uint64_t *off, const void *value, const void *cond,
                       void *fetched, void *stream);
+
+/* One atomic operation issued from the host: the per-call path behind
+ * shmem_[ctx_]<T>_atomic_<op> (shmemc_ctx_fadd & co., src/shmemc/ucx/
+ * comms.c:409-671).  value/cond are passed by value (4 or 8 bytes read from
+ * the pointers), the old value is written to *fetched (may be NULL).
+ * Blocking: one kernel launch and one stream synchronisation per call, so
+ * batch with b200shm_amo_batch wherever there is more than one. */
+int b200shm_amo(int amo, int dtype, int pe, uint64_t off, const void *value,
+                const void *cond, void *fetched);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,270 @@
+/*
+ * shmem.h -- the OpenSHMEM calls of the collective and atomic hot path,
+ * with the names, argument lists and meanings of BTMichalowicz/osss-ucx
+ * (include/shmem/api.h, include/shmem/teams.h, include/shmem/defs.h), backed
+ * by the B200 engine (libshmem_b200.so over libb200shm.so).
+ *
+ * What is here: init/finalize/my_pe/n_pes, the symmetric heap
+ * (shmem_malloc/free/calloc/align, shmem_ptr), put/get/p/g, fence/quiet,
+ * barrier_all/sync_all/barrier/sync/team_sync, the reductions
+ * (shmem_<T>_<op>_reduce and shmem_<T>_<op>_to_all over the reference's type
+ * tables), fcollect / broadcast / alltoall / alltoalls in their typed, mem
+ * and 32/64 forms, the atomics (shmem_[ctx_]<T>_atomic_*), and teams
+ * (world, split_strided, split_2d, my_pe, n_pes, translate, destroy).
+ *
+ * How PEs run: every PE is a host thread of one process, started by
+ * shmemx_b200_run (include/shmemx.h); its symmetric heap is a slice of one
+ * GPU arena (CUDA managed memory by default, so host code may read and write
+ * it directly).  A collective returns when it is complete for every member,
+ * as in the reference.  Global and static variables are NOT symmetric here
+ * (threads share them): symmetric data must come from shmem_malloc.
+ */
+#ifndef B200_SHMEM_H
+#define B200_SHMEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <sys/types.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- constants (values as in include/shmem/defs.h) -------------------- */
+enum { SHMEM_CMP_EQ = 0, SHMEM_CMP_NE, SHMEM_CMP_GT, SHMEM_CMP_LE, SHMEM_CMP_LT, SHMEM_CMP_GE };
+#define SHMEM_BCAST_SYNC_SIZE 64
+#define SHMEM_BARRIER_SYNC_SIZE 2
+#define SHMEM_REDUCE_SYNC_SIZE 128
+#define SHMEM_REDUCE_MIN_WRKDATA_SIZE 64
+#define SHMEM_COLLECT_SYNC_SIZE 128
+#define SHMEM_ALLTOALL_SYNC_SIZE 64
+#define SHMEM_ALLTOALLS_SYNC_SIZE 64
+#define SHMEM_SYNC_SIZE SHMEM_REDUCE_SYNC_SIZE
+#define SHMEM_SYNC_VALUE 0L
+#define SHMEM_THREAD_SINGLE 0
+#define SHMEM_THREAD_FUNNELED 1
+#define SHMEM_THREAD_SERIALIZED 2
+#define SHMEM_THREAD_MULTIPLE 3
+
+typedef void *shmem_team_t;
+typedef void *shmem_ctx_t;
+typedef struct {
+  int num_contexts;
+} shmem_team_config_t;
+extern shmem_team_t SHMEM_TEAM_WORLD;
+extern shmem_team_t SHMEM_TEAM_SHARED;
+extern shmem_team_t SHMEM_TEAM_INVALID;
+extern shmem_ctx_t SHMEM_CTX_DEFAULT;
+
+/* ---- setup / query ----------------------------------------------------- */
+void shmem_init(void);
+int shmem_init_thread(int requested, int *provided);
+void shmem_finalize(void);
+int shmem_my_pe(void);
+int shmem_n_pes(void);
+int shmem_pe_accessible(int pe);
+void shmem_global_exit(int status);
+
+/* ---- symmetric heap ---------------------------------------------------- */
+void *shmem_malloc(size_t size);
+void *shmem_calloc(size_t count, size_t size);
+void *shmem_align(size_t alignment, size_t size);
+void shmem_free(void *ptr);
+void *shmem_ptr(const void *dest, int pe);
+
+/* ---- RMA and ordering -------------------------------------------------- */
+void shmem_putmem(void *dest, const void *source, size_t nelems, int pe);
+void shmem_getmem(void *dest, const void *source, size_t nelems, int pe);
+void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe);
+void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe);
+void shmem_fence(void);
+void shmem_quiet(void);
+
+/* ---- synchronisation --------------------------------------------------- */
+void shmem_barrier_all(void);
+void shmem_sync_all(void);
+void shmem_barrier(int PE_start, int logPE_stride, int PE_size, long *pSync);
+void shmem_sync(int PE_start, int logPE_stride, int PE_size, long *pSync);
+int shmem_team_sync(shmem_team_t team);
+
+/* ---- teams (include/shmem/teams.h) -------------------------------------- */
+int shmem_team_my_pe(shmem_team_t team);
+int shmem_team_n_pes(shmem_team_t team);
+int shmem_team_translate_pe(shmem_team_t src_team, int src_pe, shmem_team_t dest_team);
+int shmem_team_split_strided(shmem_team_t parent_team, int start, int stride, int size,
+                             const shmem_team_config_t *config, long config_mask,
+                             shmem_team_t *new_team);
+int shmem_team_split_2d(shmem_team_t parent_team, int xrange,
+                        const shmem_team_config_t *xaxis_config, long xaxis_mask,
+                        shmem_team_t *xaxis_team, const shmem_team_config_t *yaxis_config,
+                        long yaxis_mask, shmem_team_t *yaxis_team);
+void shmem_team_destroy(shmem_team_t team);
+int shmem_team_get_config(shmem_team_t team, long config_mask, shmem_team_config_t *config);
+
+/* ---- type tables (the names of include/shmem/api_types.h) -------------- */
+#define SHMEM_B200_REDUCE_BITWISE_TYPES(X)                                      \
+  X(unsigned char, uchar) X(unsigned short, ushort) X(unsigned int, uint)       \
+  X(unsigned long, ulong) X(unsigned long long, ulonglong) X(int8_t, int8)      \
+  X(int16_t, int16) X(int32_t, int32) X(int64_t, int64) X(uint8_t, uint8)       \
+  X(uint16_t, uint16) X(uint32_t, uint32) X(uint64_t, uint64) X(size_t, size)
+#define SHMEM_B200_REDUCE_MINMAX_TYPES(X)                                       \
+  X(char, char) X(signed char, schar) X(short, short) X(int, int) X(long, long) \
+  X(long long, longlong) X(ptrdiff_t, ptrdiff) X(unsigned char, uchar)          \
+  X(unsigned short, ushort) X(unsigned int, uint) X(unsigned long, ulong)       \
+  X(unsigned long long, ulonglong) X(int8_t, int8) X(int16_t, int16)            \
+  X(int32_t, int32) X(int64_t, int64) X(uint8_t, uint8) X(uint16_t, uint16)     \
+  X(uint32_t, uint32) X(uint64_t, uint64) X(size_t, size) X(float, float)       \
+  X(double, double) X(long double, longdouble)
+#define SHMEM_B200_REDUCE_ARITH_TYPES(X)                                        \
+  SHMEM_B200_REDUCE_MINMAX_TYPES(X)                                             \
+  X(double _Complex, complexd) X(float _Complex, complexf)
+#define SHMEM_B200_TO_ALL_BITWISE_TYPES(X)                                      \
+  X(short, short) X(int, int) X(long, long) X(long long, longlong)
+#define SHMEM_B200_TO_ALL_MINMAX_TYPES(X)                                       \
+  SHMEM_B200_TO_ALL_BITWISE_TYPES(X) X(float, float) X(double, double)          \
+  X(long double, longdouble)
+#define SHMEM_B200_TO_ALL_ARITH_TYPES(X)                                        \
+  SHMEM_B200_TO_ALL_MINMAX_TYPES(X) X(double _Complex, complexd)                \
+  X(float _Complex, complexf)
+#define SHMEM_B200_RMA_TYPES(X)                                                 \
+  X(float, float) X(double, double) X(long double, longdouble) X(char, char)    \
+  X(signed char, schar) X(short, short) X(int, int) X(long, long)               \
+  X(long long, longlong) X(unsigned char, uchar) X(unsigned short, ushort)      \
+  X(unsigned int, uint) X(unsigned long, ulong) X(unsigned long long, ulonglong) \
+  X(int8_t, int8) X(int16_t, int16) X(int32_t, int32) X(int64_t, int64)         \
+  X(uint8_t, uint8) X(uint16_t, uint16) X(uint32_t, uint32) X(uint64_t, uint64) \
+  X(size_t, size) X(ptrdiff_t, ptrdiff)
+#define SHMEM_B200_AMO_STANDARD_TYPES(X)                                        \
+  X(int, int) X(long, long) X(long long, longlong) X(unsigned int, uint)        \
+  X(unsigned long, ulong) X(unsigned long long, ulonglong) X(int32_t, int32)    \
+  X(int64_t, int64) X(uint32_t, uint32) X(uint64_t, uint64) X(size_t, size)     \
+  X(ptrdiff_t, ptrdiff)
+#define SHMEM_B200_AMO_EXTENDED_TYPES(X)                                        \
+  X(float, float) X(double, double) SHMEM_B200_AMO_STANDARD_TYPES(X)
+#define SHMEM_B200_AMO_BITWISE_TYPES(X)                                         \
+  X(unsigned int, uint) X(unsigned long, ulong) X(unsigned long long, ulonglong) \
+  X(int32_t, int32) X(int64_t, int64) X(uint32_t, uint32) X(uint64_t, uint64)
+
+/* ---- reductions: team form (reduce.c:1078-1102) and active-set form ---- */
+#define SHMEM_B200_DECL_REDUCE(_op)                                             \
+  SHMEM_B200_DECL_REDUCE_##_op
+#define SHMEM_B200_DECL_TEAM_REDUCE(_type, _tn, _op)                            \
+  int shmem_##_tn##_##_op##_reduce(shmem_team_t team, _type *dest,             \
+                                   const _type *source, size_t nreduce);
+#define SHMEM_B200_DECL_TO_ALL(_type, _tn, _op)                                 \
+  void shmem_##_tn##_##_op##_to_all(_type *dest, const _type *source,          \
+                                    int nreduce, int PE_start,                  \
+                                    int logPE_stride, int PE_size,              \
+                                    _type *pWrk, long *pSync);
+#define SHMEM_B200_D_AND(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, and)
+#define SHMEM_B200_D_OR(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, or)
+#define SHMEM_B200_D_XOR(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, xor)
+#define SHMEM_B200_D_MIN(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, min)
+#define SHMEM_B200_D_MAX(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, max)
+#define SHMEM_B200_D_SUM(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, sum)
+#define SHMEM_B200_D_PROD(_t, _n) SHMEM_B200_DECL_TEAM_REDUCE(_t, _n, prod)
+SHMEM_B200_REDUCE_BITWISE_TYPES(SHMEM_B200_D_AND)
+SHMEM_B200_REDUCE_BITWISE_TYPES(SHMEM_B200_D_OR)
+SHMEM_B200_REDUCE_BITWISE_TYPES(SHMEM_B200_D_XOR)
+SHMEM_B200_REDUCE_MINMAX_TYPES(SHMEM_B200_D_MIN)
+SHMEM_B200_REDUCE_MINMAX_TYPES(SHMEM_B200_D_MAX)
+SHMEM_B200_REDUCE_ARITH_TYPES(SHMEM_B200_D_SUM)
+SHMEM_B200_REDUCE_ARITH_TYPES(SHMEM_B200_D_PROD)
+#define SHMEM_B200_T_AND(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, and)
+#define SHMEM_B200_T_OR(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, or)
+#define SHMEM_B200_T_XOR(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, xor)
+#define SHMEM_B200_T_MIN(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, min)
+#define SHMEM_B200_T_MAX(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, max)
+#define SHMEM_B200_T_SUM(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, sum)
+#define SHMEM_B200_T_PROD(_t, _n) SHMEM_B200_DECL_TO_ALL(_t, _n, prod)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(SHMEM_B200_T_AND)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(SHMEM_B200_T_OR)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(SHMEM_B200_T_XOR)
+SHMEM_B200_TO_ALL_MINMAX_TYPES(SHMEM_B200_T_MIN)
+SHMEM_B200_TO_ALL_MINMAX_TYPES(SHMEM_B200_T_MAX)
+SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_SUM)
+SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_PROD)
+
+/* ---- data movement (shcoll-shim.c:185-702) ------------------------------ */
+#define SHMEM_B200_DECL_COPY(_type, _tn)                                        \
+  int shmem_##_tn##_fcollect(shmem_team_t team, _type *dest,                   \
+                             const _type *source, size_t nelems);               \
+  int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                   \
+                             const _type *source, size_t nelems);               \
+  int shmem_##_tn##_alltoalls(shmem_team_t team, _type *dest,                  \
+                              const _type *source, ptrdiff_t dst,               \
+                              ptrdiff_t sst, size_t nelems);                    \
+  int shmem_##_tn##_broadcast(shmem_team_t team, _type *dest,                  \
+                              const _type *source, size_t nelems, int PE_root); \
+  void shmem_##_tn##_put(_type *dest, const _type *source, size_t nelems,      \
+                         int pe);                                               \
+  void shmem_##_tn##_get(_type *dest, const _type *source, size_t nelems,      \
+                         int pe);                                               \
+  void shmem_##_tn##_p(_type *dest, _type value, int pe);                      \
+  _type shmem_##_tn##_g(const _type *source, int pe);
+SHMEM_B200_RMA_TYPES(SHMEM_B200_DECL_COPY)
+int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
+int shmem_alltoallmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
+int shmem_alltoallsmem(shmem_team_t team, void *dest, const void *source, ptrdiff_t dst,
+                       ptrdiff_t sst, size_t nelems);
+int shmem_broadcastmem(shmem_team_t team, void *dest, const void *source, size_t nelems,
+                       int PE_root);
+void shmem_fcollect32(void *target, const void *source, size_t nelems, int PE_start,
+                      int logPE_stride, int PE_size, long *pSync);
+void shmem_fcollect64(void *target, const void *source, size_t nelems, int PE_start,
+                      int logPE_stride, int PE_size, long *pSync);
+void shmem_alltoall32(void *target, const void *source, size_t nelems, int PE_start,
+                      int logPE_stride, int PE_size, long *pSync);
+void shmem_alltoall64(void *target, const void *source, size_t nelems, int PE_start,
+                      int logPE_stride, int PE_size, long *pSync);
+void shmem_alltoalls32(void *target, const void *source, ptrdiff_t dst, ptrdiff_t sst,
+                       size_t nelems, int PE_start, int logPE_stride, int PE_size, long *pSync);
+void shmem_alltoalls64(void *target, const void *source, ptrdiff_t dst, ptrdiff_t sst,
+                       size_t nelems, int PE_start, int logPE_stride, int PE_size, long *pSync);
+void shmem_broadcast32(void *target, const void *source, size_t nelems, int PE_root,
+                       int PE_start, int logPE_stride, int PE_size, long *pSync);
+void shmem_broadcast64(void *target, const void *source, size_t nelems, int PE_root,
+                       int PE_start, int logPE_stride, int PE_size, long *pSync);
+
+/* ---- atomics (the files of src/api/atomics) ----------------------------- */
+#define SHMEM_B200_DECL_AMO_STD(_type, _tn)                                     \
+  _type shmem_##_tn##_atomic_fetch_add(_type *dest, _type value, int pe);      \
+  void shmem_##_tn##_atomic_add(_type *dest, _type value, int pe);             \
+  _type shmem_##_tn##_atomic_fetch_inc(_type *dest, int pe);                   \
+  void shmem_##_tn##_atomic_inc(_type *dest, int pe);                          \
+  _type shmem_##_tn##_atomic_compare_swap(_type *dest, _type cond,             \
+                                          _type value, int pe);                 \
+  _type shmem_ctx_##_tn##_atomic_fetch_add(shmem_ctx_t ctx, _type *dest,       \
+                                           _type value, int pe);                \
+  void shmem_ctx_##_tn##_atomic_add(shmem_ctx_t ctx, _type *dest, _type value, \
+                                    int pe);                                    \
+  _type shmem_ctx_##_tn##_atomic_fetch_inc(shmem_ctx_t ctx, _type *dest,       \
+                                           int pe);                             \
+  void shmem_ctx_##_tn##_atomic_inc(shmem_ctx_t ctx, _type *dest, int pe);     \
+  _type shmem_ctx_##_tn##_atomic_compare_swap(shmem_ctx_t ctx, _type *dest,    \
+                                              _type cond, _type value, int pe);
+#define SHMEM_B200_DECL_AMO_EXT(_type, _tn)                                     \
+  _type shmem_##_tn##_atomic_swap(_type *dest, _type value, int pe);           \
+  void shmem_##_tn##_atomic_set(_type *dest, _type value, int pe);             \
+  _type shmem_##_tn##_atomic_fetch(const _type *source, int pe);               \
+  _type shmem_ctx_##_tn##_atomic_swap(shmem_ctx_t ctx, _type *dest,            \
+                                      _type value, int pe);                     \
+  void shmem_ctx_##_tn##_atomic_set(shmem_ctx_t ctx, _type *dest, _type value, \
+                                    int pe);                                    \
+  _type shmem_ctx_##_tn##_atomic_fetch(shmem_ctx_t ctx, const _type *source,   \
+                                       int pe);
+#define SHMEM_B200_DECL_AMO_BIT(_type, _tn)                                     \
+  _type shmem_##_tn##_atomic_fetch_and(_type *dest, _type value, int pe);      \
+  _type shmem_##_tn##_atomic_fetch_or(_type *dest, _type value, int pe);       \
+  _type shmem_##_tn##_atomic_fetch_xor(_type *dest, _type value, int pe);      \
+  void shmem_##_tn##_atomic_and(_type *dest, _type value, int pe);             \
+  void shmem_##_tn##_atomic_or(_type *dest, _type value, int pe);              \
+  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe);
+SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_STD)
+SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_EXT)
+SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -22,6 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 CUDA_LIB = "libb200shm.so"
+HOST_LIB = "libshmem_b200.so"
+CC = os.environ.get("CC", "gcc")
 
 
 def _stale(target, deps):
@@ -52,6 +54,7 @@ def build(verbose=False, extra=()):
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
     lib = os.path.join(LIB, CUDA_LIB)
     if not extra and not _stale(lib, srcs + heads + [__file__]):
+        build_host(lib)
         return lib  # up to date (objects may be absent, e.g. in a shipped snapshot)
     jobs = []
     objs = []
@@ -69,7 +72,24 @@ def build(verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    build_host(lib)
     return lib
+
+
+def build_host(cuda_lib=None):
+    """The OpenSHMEM surface (include/shmem.h) in C over libb200shm.so."""
+    cuda_lib = cuda_lib or os.path.join(LIB, CUDA_LIB)
+    srcs = sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".c"))
+    out = os.path.join(LIB, HOST_LIB)
+    heads = [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    if not _stale(out, srcs + heads + [cuda_lib, __file__]):
+        return out
+    cmd = [CC, "-std=gnu11", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-unused-function",
+           "-o", out] + srcs + ["-L" + LIB, "-lb200shm", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("host library build failed:\n" + r.stdout + r.stderr)
+    return out
 
 
 if __name__ == "__main__":

@@ -14,6 +14,9 @@
  * alignment); an invalid one is skipped and sets the BADREQ status bit.
  */
 #include <stdint.h>
+#include <string.h>
+
+#include <mutex>
 
 #include "internal.cuh"
 
@@ -60,6 +63,15 @@ __global__ void __launch_bounds__(256) k_amo(int amo, uint64_t nops, const int32
   }
 }
 
+/* one operation, operands by value; the old value goes to mapped host
+ * memory so the caller reads it right after the stream synchronises */
+template <class W>
+__global__ void k_amo_one(int amo, W *target, W v, W c, W *fetched, int ok) {
+  if (!ok) return;
+  const W old = amo_one<W>(amo, target, v, c);
+  if (fetched) *fetched = old;
+}
+
 }  // namespace
 
 int amo_launch(int amo, int dtype, uint64_t nops, const int32_t *pe, const uint64_t *off,
@@ -99,4 +111,64 @@ extern "C" int b200shm_amo_batch(int amo, int dtype, uint64_t nops, const int32_
   int rc = b200::amo_launch(amo, dtype, nops, pe, off, value, cond, fetched,
                             b200::pick_stream(stream));
   return rc ? rc : b200::finish(stream, "b200shm_amo_batch");
+}
+
+/* Per-thread slot of mapped pinned memory for b200shm_amo's fetched value. */
+namespace b200 {
+static int amo_slot(unsigned long long **host, unsigned long long **dev) {
+  static std::mutex mu;
+  static unsigned long long *h = nullptr, *d = nullptr;
+  static int next = 0;
+  static thread_local int mine = -1;
+  constexpr int kSlots = 4096;
+  std::lock_guard<std::mutex> lk(mu);
+  if (h == nullptr) {
+    cudaError_t e = cudaHostAlloc((void **)&h, kSlots * 64, cudaHostAllocMapped);
+    if (e != cudaSuccess) return cuda_fail(e, "b200shm_amo slot");
+    e = cudaHostGetDevicePointer((void **)&d, h, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "b200shm_amo slot");
+  }
+  if (mine < 0) mine = (next++) % kSlots;
+  *host = h + (size_t)mine * 8;
+  *dev = d + (size_t)mine * 8;
+  return B200SHM_OK;
+}
+}  // namespace b200
+
+extern "C" int b200shm_amo(int amo, int dtype, int pe, uint64_t off, const void *value,
+                           const void *cond, void *fetched) {
+  using namespace b200;
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (amo < 0 || amo >= B200SHM_AMO_NOP) return fail(B200SHM_ERR_ARG, "amo: unknown op %d", amo);
+  const bool w4 = dtype == B200SHM_I32 || dtype == B200SHM_U32 || dtype == B200SHM_F32;
+  const bool w8 = dtype == B200SHM_I64 || dtype == B200SHM_U64 || dtype == B200SHM_F64;
+  if (!w4 && !w8) return fail(B200SHM_ERR_UNSUPPORTED, "amo: dtype %d is not 4 or 8 bytes", dtype);
+  const bool is_float = dtype == B200SHM_F32 || dtype == B200SHM_F64;
+  if (is_float && amo != B200SHM_AMO_SWAP && amo != B200SHM_AMO_SET && amo != B200SHM_AMO_FETCH)
+    return fail(B200SHM_ERR_UNSUPPORTED, "amo: floating types support only swap/set/fetch");
+  const uint64_t w = w8 ? 8 : 4;
+  if (pe < 0 || pe >= st().npes || off > st().slice - w || off % w)
+    return fail(B200SHM_ERR_ARG, "amo: target (PE %d, offset %llu) is not a %llu-byte word of the heap",
+                pe, (unsigned long long)off, (unsigned long long)w);
+  unsigned long long *h = nullptr, *d = nullptr;
+  int rc = amo_slot(&h, &d);
+  if (rc) return rc;
+  char *target = st().base + (uint64_t)pe * st().slice + off;
+  cudaStream_t s = st().stream;
+  if (w8) {
+    unsigned long long v = 0, c = 0;
+    if (value) memcpy(&v, value, 8);
+    if (cond) memcpy(&c, cond, 8);
+    k_amo_one<unsigned long long><<<1, 1, 0, s>>>(amo, (unsigned long long *)target, v, c, d, 1);
+  } else {
+    unsigned int v = 0, c = 0;
+    if (value) memcpy(&v, value, 4);
+    if (cond) memcpy(&c, cond, 4);
+    k_amo_one<unsigned int><<<1, 1, 0, s>>>(amo, (unsigned int *)target, v, c, (unsigned int *)d, 1);
+  }
+  count_launch();
+  rc = finish(nullptr, "b200shm_amo");
+  if (rc) return rc;
+  if (fetched) memcpy(fetched, (const void *)h, w);
+  return B200SHM_OK;
 }

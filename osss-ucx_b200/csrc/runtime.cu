@@ -293,6 +293,14 @@ int b200shm_get_host(void *host_dst, int pe_start, int pe_stride, int pe_count, 
   return finish(stream, "b200shm_get_host");
 }
 
+int b200shm_memcpy(void *dst, const void *src, uint64_t bytes, void *stream) {
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (bytes == 0) return B200SHM_OK;
+  if (!dst || !src) return fail(B200SHM_ERR_ARG, "memcpy: null pointer");
+  B200_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, pick_stream(stream)));
+  return finish(stream, "b200shm_memcpy");
+}
+
 int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off, int byte,
                    uint64_t bytes_per_pe, void *stream) {
   int rc = check_team(pe_start, pe_stride, pe_count);

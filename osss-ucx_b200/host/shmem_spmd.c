@@ -1,0 +1,826 @@
+/*
+ * shmem_spmd.c -- the OpenSHMEM calls of the collective and atomic hot path
+ * (include/shmem.h), for SPMD programs whose PEs are host threads, backed by
+ * the B200 engine (include/b200shm.h).
+ *
+ * In the reference every PE is an OS process and every collective runs its
+ * algorithm as rounds of UCX puts between them (src/shcoll/src, reached via
+ * src/api/collectives/shcoll-shim.c).  Here every PE is a thread started by
+ * shmemx_b200_run, all symmetric heaps are slices of one GPU arena, and a
+ * collective is ONE device call for the whole team: each team (and each
+ * active set of the deprecated forms) has an arrival point; members record
+ * their arguments there, the last to arrive checks that every member passed
+ * the same symmetric offsets and counts and issues the b200shm_* call, and
+ * all members return when it has completed -- so every collective is also a
+ * barrier among its members, as in the reference.
+ *
+ * Algorithm names are read from the reference's environment variables
+ * (src/shmemc/env.c:186-312): SHMEM_<OP>_REDUCE_ALGO / SHMEM_<OP>_TO_ALL_ALGO
+ * choose the combine order (linear, binomial, rec_dbl, rabenseifner,
+ * rabenseifner2; default rec_dbl, src/api/collectives/defaults.h) and
+ * SHMEM_BARRIER[_ALL]_ALGO, SHMEM_SYNC[_ALL]_ALGO, SHMEM_TEAM_SYNC_ALGO the
+ * barrier pattern (default binomial_tree).  fcollect / alltoall(s) /
+ * broadcast produce the same bytes whatever their algorithm name, so those
+ * names are accepted and ignored.
+ */
+#include <errno.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "../../include/b200shm.h"
+#include "../../include/shmem.h"
+#include "../../include/shmemx.h"
+
+/* ---- errors ---------------------------------------------------------------- */
+static __thread char t_err[512];
+static __thread int t_status;
+
+static int set_err(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_err, sizeof(t_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+const char *shmemx_b200_last_error(void) { return t_err[0] ? t_err : b200shm_last_error(); }
+int shmemx_b200_last_status(void) { return t_status; }
+static int engine_err(int rc) {
+  if (rc) set_err(rc, "%s", b200shm_last_error());
+  return rc;
+}
+
+double shmemx_wtime(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* ---- PEs -------------------------------------------------------------------- */
+static int g_npes;           /* PEs of the running job (world size) */
+static char *g_base;         /* arena base */
+static uint64_t g_slice;     /* bytes per PE slice */
+static uint64_t g_scratch;   /* per-PE scratch offset (AMO operands) */
+static __thread int t_pe = -1;
+
+/* ---- arrival points ----------------------------------------------------- */
+enum { K_NONE, K_MALLOC, K_FREE, K_BARRIER, K_REDUCE, K_FCOLLECT, K_ALLTOALL, K_ALLTOALLS,
+       K_BROADCAST, K_SPLIT, K_SPLIT2D, K_DESTROY };
+
+typedef struct coll {
+  int kind, op, dtype, algo, root;
+  uint64_t dest, src, n, esize;
+  int64_t a, b;
+} coll_t;
+
+typedef struct agg {
+  pthread_mutex_t mu;
+  pthread_cond_t cv;
+  int arrived, mismatch, rc;
+  unsigned long gen;
+  coll_t req;
+  uint64_t out;
+  void *outp, *outq;
+} agg_t;
+
+typedef struct b200_team {
+  int start, stride, size; /* global PEs start + i*stride, i < size */
+  int valid;
+  agg_t agg;
+  struct b200_team *next; /* every team ever made, freed at exit */
+} b200_team_t;
+
+static b200_team_t g_world;
+static pthread_mutex_t g_teams_mu = PTHREAD_MUTEX_INITIALIZER;
+static b200_team_t *g_teams;    /* split teams */
+static b200_team_t *g_actsets;  /* arrival points of the active-set forms */
+
+shmem_team_t SHMEM_TEAM_WORLD = &g_world;
+shmem_team_t SHMEM_TEAM_SHARED = &g_world;
+shmem_team_t SHMEM_TEAM_INVALID = NULL;
+shmem_ctx_t SHMEM_CTX_DEFAULT = NULL;
+
+static void agg_init(agg_t *g) {
+  pthread_mutex_init(&g->mu, NULL);
+  pthread_cond_init(&g->cv, NULL);
+  g->arrived = g->mismatch = g->rc = 0;
+  g->gen = 0;
+}
+
+static b200_team_t *team_new(int start, int stride, int size) {
+  b200_team_t *t = (b200_team_t *)calloc(1, sizeof(*t));
+  if (!t) return NULL;
+  t->start = start;
+  t->stride = size > 1 ? stride : 1;
+  t->size = size;
+  t->valid = 1;
+  agg_init(&t->agg);
+  pthread_mutex_lock(&g_teams_mu);
+  t->next = g_teams;
+  g_teams = t;
+  pthread_mutex_unlock(&g_teams_mu);
+  return t;
+}
+
+/* index of global PE `pe` in team t, or -1 */
+static int team_index(const b200_team_t *t, int pe) {
+  if (!t || !t->valid || pe < t->start) return -1;
+  const int d = pe - t->start;
+  if (d % t->stride) return -1;
+  return d / t->stride < t->size ? d / t->stride : -1;
+}
+
+/* arrival point of the active set (PE_start, 2^logPE_stride, PE_size) */
+static b200_team_t *active_set(int start, int logstride, int size) {
+  const int stride = 1 << logstride;
+  pthread_mutex_lock(&g_teams_mu);
+  b200_team_t *t = g_actsets;
+  for (; t; t = t->next)
+    if (t->start == start && t->stride == (size > 1 ? stride : 1) && t->size == size) break;
+  if (!t) {
+    t = (b200_team_t *)calloc(1, sizeof(*t));
+    if (t) {
+      t->start = start;
+      t->stride = size > 1 ? stride : 1;
+      t->size = size;
+      t->valid = 1;
+      agg_init(&t->agg);
+      t->next = g_actsets;
+      g_actsets = t;
+    }
+  }
+  pthread_mutex_unlock(&g_teams_mu);
+  return t;
+}
+
+static int same_req(const coll_t *x, const coll_t *y) {
+  return x->kind == y->kind && x->op == y->op && x->dtype == y->dtype && x->algo == y->algo &&
+         x->root == y->root && x->dest == y->dest && x->src == y->src && x->n == y->n &&
+         x->esize == y->esize && x->a == y->a && x->b == y->b;
+}
+
+static int launch(b200_team_t *t, agg_t *g);
+
+/* Record this member's arguments; the last member to arrive launches. */
+static int arrive(b200_team_t *t, const coll_t *mine) {
+  if (t_pe < 0) return set_err(B200SHM_ERR_STATE, "not a PE thread (start PEs with shmemx_b200_run)");
+  if (!t || !t->valid) return set_err(B200SHM_ERR_ARG, "invalid team");
+  if (team_index(t, t_pe) < 0)
+    return set_err(B200SHM_ERR_ARG, "PE %d is not a member of the team/active set", t_pe);
+  agg_t *g = &t->agg;
+  pthread_mutex_lock(&g->mu);
+  const unsigned long gen = g->gen;
+  if (g->arrived == 0) {
+    g->req = *mine;
+    g->mismatch = 0;
+  } else if (!same_req(&g->req, mine)) {
+    g->mismatch = 1;
+  }
+  if (++g->arrived == t->size) {
+    g->rc = g->mismatch ? set_err(B200SHM_ERR_ARG,
+                                  "members passed different arguments (non-symmetric "
+                                  "addresses or counts)")
+                        : launch(t, g);
+    g->arrived = 0;
+    g->gen++;
+    pthread_cond_broadcast(&g->cv);
+  } else {
+    while (gen == g->gen) pthread_cond_wait(&g->cv, &g->mu);
+  }
+  const int rc = g->rc;
+  pthread_mutex_unlock(&g->mu);
+  t_status = rc;
+  if (rc && !t_err[0]) set_err(rc, "%s", b200shm_last_error());
+  return rc;
+}
+
+/* ---- algorithm names ------------------------------------------------------ */
+static int parse_algo(const char *env, const char *const *names, int n, int dflt) {
+  const char *e = getenv(env);
+  if (!e || !*e) return dflt;
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%s", e);
+  char *colon = strchr(buf, ':'); /* "rec_dbl:int32" names a typed entry */
+  if (colon) *colon = 0;
+  for (int i = 0; i < n; i++)
+    if (strcmp(buf, names[i]) == 0) return i;
+  fprintf(stderr, "shmem_b200: unknown %s=%s, using the default\n", env, e);
+  return dflt;
+}
+static const char *const k_reduce_names[] = {"linear", "binomial", "rec_dbl", "rabenseifner",
+                                             "rabenseifner2"};
+static const char *const k_barrier_names[] = {"linear", "complete_tree", "binomial_tree",
+                                              "knomial_tree", "dissemination"};
+static const char *const k_op_env[] = {"AND", "OR", "XOR", "MIN", "MAX", "SUM", "PROD"};
+static int g_reduce_algo[2][7]; /* [0] team form, [1] to_all form */
+static int g_barrier_algo, g_barrier_all_algo, g_sync_algo, g_sync_all_algo, g_team_sync_algo;
+
+static void read_env(void) {
+  char name[64];
+  for (int op = 0; op < 7; op++) {
+    snprintf(name, sizeof(name), "SHMEM_%s_REDUCE_ALGO", k_op_env[op]);
+    g_reduce_algo[0][op] = parse_algo(name, k_reduce_names, 5, B200SHM_REC_DBL);
+    snprintf(name, sizeof(name), "SHMEM_%s_TO_ALL_ALGO", k_op_env[op]);
+    g_reduce_algo[1][op] = parse_algo(name, k_reduce_names, 5, B200SHM_REC_DBL);
+  }
+  g_barrier_algo = parse_algo("SHMEM_BARRIER_ALGO", k_barrier_names, 5, B200SHM_BAR_BINOMIAL_TREE);
+  g_barrier_all_algo = parse_algo("SHMEM_BARRIER_ALL_ALGO", k_barrier_names, 5, B200SHM_BAR_BINOMIAL_TREE);
+  g_sync_algo = parse_algo("SHMEM_SYNC_ALGO", k_barrier_names, 5, B200SHM_BAR_BINOMIAL_TREE);
+  g_sync_all_algo = parse_algo("SHMEM_SYNC_ALL_ALGO", k_barrier_names, 5, B200SHM_BAR_BINOMIAL_TREE);
+  g_team_sync_algo = parse_algo("SHMEM_TEAM_SYNC_ALGO", k_barrier_names, 5, B200SHM_BAR_BINOMIAL_TREE);
+}
+
+/* ---- the single device call of a collective -------------------------------- */
+static int launch(b200_team_t *t, agg_t *g) {
+  const coll_t *r = &g->req;
+  switch (r->kind) {
+  case K_MALLOC: {
+    uint64_t off = 0;
+    int rc = b200shm_malloc(r->n, r->a, &off);
+    g->out = off;
+    return engine_err(rc);
+  }
+  case K_FREE: return engine_err(b200shm_free(r->dest));
+  case K_BARRIER: return engine_err(b200shm_barrier(r->algo, t->start, t->stride, t->size, NULL));
+  case K_REDUCE:
+    return engine_err(b200shm_reduce(r->op, r->dtype, r->algo, t->start, t->stride, t->size,
+                                     r->dest, r->src, r->n, NULL));
+  case K_FCOLLECT:
+    return engine_err(b200shm_fcollect(t->start, t->stride, t->size, r->dest, r->src, r->n, NULL));
+  case K_ALLTOALL:
+    return engine_err(b200shm_alltoall(t->start, t->stride, t->size, r->dest, r->src, r->n, NULL));
+  case K_ALLTOALLS:
+    return engine_err(b200shm_alltoalls(t->start, t->stride, t->size, r->dest, r->src, r->a, r->b,
+                                        r->n, r->esize, NULL));
+  case K_BROADCAST:
+    return engine_err(b200shm_broadcast(r->root, t->start, t->stride, t->size, r->dest, r->src,
+                                        r->n, NULL));
+  case K_SPLIT: { /* (start, stride, size) relative to the parent team */
+    const int start = (int)r->a, stride = (int)r->b, size = (int)r->n;
+    if (size < 1 || start < 0 || (size > 1 && stride < 1) ||
+        start + (int64_t)(size - 1) * (size > 1 ? stride : 0) >= t->size)
+      return set_err(B200SHM_ERR_ARG, "team_split_strided: (%d, %d, %d) outside the parent", start,
+                     stride, size);
+    b200_team_t *n = team_new(t->start + start * t->stride, t->stride * (size > 1 ? stride : 1), size);
+    g->outp = n;
+    return n ? 0 : set_err(B200SHM_ERR_NOMEM, "team_split_strided: out of memory");
+  }
+  case K_SPLIT2D: { /* x teams: runs of xrange members; y teams: members with equal i%xrange */
+    const int xr = (int)r->a, n = t->size;
+    if (xr < 1) return set_err(B200SHM_ERR_ARG, "team_split_2d: xrange %d < 1", xr);
+    const int nx = (n + xr - 1) / xr, ny = xr < n ? xr : n;
+    b200_team_t **xs = (b200_team_t **)calloc((size_t)nx, sizeof(*xs));
+    b200_team_t **ys = (b200_team_t **)calloc((size_t)ny, sizeof(*ys));
+    if (!xs || !ys) return set_err(B200SHM_ERR_NOMEM, "team_split_2d: out of memory");
+    for (int k = 0; k < nx; k++) {
+      const int sz = (n - k * xr) < xr ? (n - k * xr) : xr;
+      xs[k] = team_new(t->start + k * xr * t->stride, t->stride, sz);
+    }
+    for (int j = 0; j < ny; j++)
+      ys[j] = team_new(t->start + j * t->stride, t->stride * xr, (n - j + xr - 1) / xr);
+    g->outp = xs;
+    g->outq = ys;
+    return 0;
+  }
+  case K_DESTROY: t->valid = 0; return 0;
+  default: return set_err(B200SHM_ERR_ARG, "unknown collective");
+  }
+}
+
+/* ---- symmetric addresses ------------------------------------------------- */
+static int sym_off(const void *p, uint64_t *off) {
+  const char *mine = g_base + (uint64_t)t_pe * g_slice;
+  if ((const char *)p < mine || (const char *)p >= mine + g_slice)
+    return set_err(B200SHM_ERR_ARG, "address %p is not in PE %d's symmetric heap", p, t_pe);
+  *off = (uint64_t)((const char *)p - mine);
+  return 0;
+}
+
+/* ---- start-up --------------------------------------------------------------- */
+static uint64_t parse_size(const char *s, uint64_t dflt) {
+  if (!s || !*s) return dflt;
+  char *end = NULL;
+  double v = strtod(s, &end);
+  if (end && *end) {
+    switch (*end) {
+    case 'k': case 'K': v *= 1024.0; break;
+    case 'm': case 'M': v *= 1024.0 * 1024.0; break;
+    case 'g': case 'G': v *= 1024.0 * 1024.0 * 1024.0; break;
+    default: break;
+    }
+  }
+  return v > 0 ? (uint64_t)v : dflt;
+}
+
+static int engine_up(int npes) {
+  if (b200shm_initialized()) {
+    if (b200shm_n_pes() < npes)
+      return set_err(B200SHM_ERR_STATE, "engine already started with %d PEs (< %d)",
+                     b200shm_n_pes(), npes);
+  } else {
+    const uint64_t heap = parse_size(getenv("SHMEM_SYMMETRIC_SIZE"), 64ull << 20);
+    const char *kind = getenv("SHMEM_B200_HEAP");
+    const int flags = (kind && strcmp(kind, "device") == 0) ? 0 : B200SHM_INIT_MANAGED;
+    int rc = b200shm_init(npes, heap, flags);
+    if (rc) return engine_err(rc);
+    uint64_t off = 0;
+    if ((rc = b200shm_malloc(256, 256, &off))) return engine_err(rc);
+    g_scratch = off;
+  }
+  g_base = (char *)b200shm_heap_base();
+  g_slice = b200shm_heap_slice();
+  g_npes = npes;
+  g_world.start = 0;
+  g_world.stride = 1;
+  g_world.size = npes;
+  g_world.valid = 1;
+  agg_init(&g_world.agg);
+  read_env();
+  return 0;
+}
+
+struct pe_arg {
+  void (*fn)(void *);
+  void *arg;
+  int pe;
+};
+static void *pe_trampoline(void *p) {
+  struct pe_arg *a = (struct pe_arg *)p;
+  t_pe = a->pe;
+  t_err[0] = 0;
+  a->fn(a->arg);
+  return NULL;
+}
+
+int shmemx_b200_run(int npes, void (*pe_main)(void *), void *arg) {
+  if (npes < 1 || !pe_main) return set_err(B200SHM_ERR_ARG, "shmemx_b200_run: bad arguments");
+  int rc = engine_up(npes);
+  if (rc) return rc;
+  pthread_t *th = (pthread_t *)calloc((size_t)npes, sizeof(*th));
+  struct pe_arg *args = (struct pe_arg *)calloc((size_t)npes, sizeof(*args));
+  if (!th || !args) return set_err(B200SHM_ERR_NOMEM, "shmemx_b200_run: out of memory");
+  for (int p = 0; p < npes; p++) {
+    args[p].fn = pe_main;
+    args[p].arg = arg;
+    args[p].pe = p;
+    if (pthread_create(&th[p], NULL, pe_trampoline, &args[p]) != 0)
+      return set_err(B200SHM_ERR_STATE, "shmemx_b200_run: cannot start PE %d", p);
+  }
+  for (int p = 0; p < npes; p++) pthread_join(th[p], NULL);
+  free(th);
+  free(args);
+  return 0;
+}
+
+/* ---- setup / query ----------------------------------------------------------- */
+void shmem_init(void) {
+  if (t_pe >= 0) return; /* PE threads are set up by shmemx_b200_run */
+  if (engine_up(1) == 0) t_pe = 0; /* a lone thread becomes a 1-PE job */
+}
+int shmem_init_thread(int requested, int *provided) {
+  shmem_init();
+  if (provided) *provided = requested;
+  return t_pe >= 0 ? 0 : -1;
+}
+void shmem_finalize(void) { shmem_barrier_all(); }
+int shmem_my_pe(void) { return t_pe; }
+int shmem_n_pes(void) { return g_npes; }
+int shmem_pe_accessible(int pe) { return pe >= 0 && pe < g_npes; }
+void shmem_global_exit(int status) { exit(status); }
+
+/* ---- symmetric heap ---------------------------------------------------------- */
+void *shmem_align(size_t alignment, size_t size) {
+  coll_t r = {0};
+  r.kind = K_MALLOC;
+  r.n = size;
+  r.a = (int64_t)(alignment ? alignment : 256);
+  if (arrive(&g_world, &r)) return NULL;
+  return g_base + (uint64_t)t_pe * g_slice + g_world.agg.out;
+}
+void *shmem_malloc(size_t size) { return shmem_align(256, size); }
+void *shmem_calloc(size_t count, size_t size) {
+  char *p = (char *)shmem_malloc(count * size);
+  if (p) {
+    const uint64_t off = (uint64_t)(p - (g_base + (uint64_t)t_pe * g_slice));
+    b200shm_memset(t_pe, 1, 1, off, 0, count * size, NULL);
+    shmem_barrier_all();
+  }
+  return p;
+}
+void shmem_free(void *ptr) {
+  if (!ptr) return;
+  coll_t r = {0};
+  r.kind = K_FREE;
+  if (sym_off(ptr, &r.dest)) return;
+  arrive(&g_world, &r);
+}
+void *shmem_ptr(const void *dest, int pe) {
+  uint64_t off;
+  if (sym_off(dest, &off) || pe < 0 || pe >= g_npes) return NULL;
+  return b200shm_ptr(pe, off);
+}
+
+/* ---- RMA ----------------------------------------------------------------------- */
+void shmem_putmem(void *dest, const void *source, size_t nelems, int pe) {
+  uint64_t off;
+  if (sym_off(dest, &off) == 0) t_status = engine_err(b200shm_memcpy(b200shm_ptr(pe, off), source, nelems, NULL));
+}
+void shmem_getmem(void *dest, const void *source, size_t nelems, int pe) {
+  uint64_t off;
+  if (sym_off(source, &off) == 0) t_status = engine_err(b200shm_memcpy(dest, b200shm_ptr(pe, off), nelems, NULL));
+}
+void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
+  shmem_putmem(dest, source, nelems, pe);
+}
+void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
+  shmem_getmem(dest, source, nelems, pe);
+}
+void shmem_fence(void) { b200shm_quiet(); }
+void shmem_quiet(void) { b200shm_quiet(); }
+
+#define DEF_RMA(_type, _tn)                                                    \
+  void shmem_##_tn##_put(_type *dest, const _type *source, size_t nelems,     \
+                         int pe) {                                             \
+    shmem_putmem(dest, source, nelems * sizeof(_type), pe);                    \
+  }                                                                            \
+  void shmem_##_tn##_get(_type *dest, const _type *source, size_t nelems,     \
+                         int pe) {                                             \
+    shmem_getmem(dest, source, nelems * sizeof(_type), pe);                    \
+  }                                                                            \
+  void shmem_##_tn##_p(_type *dest, _type value, int pe) {                    \
+    shmem_putmem(dest, &value, sizeof(_type), pe);                             \
+  }                                                                            \
+  _type shmem_##_tn##_g(const _type *source, int pe) {                        \
+    _type v;                                                                   \
+    memset(&v, 0, sizeof(v));                                                  \
+    shmem_getmem(&v, source, sizeof(_type), pe);                               \
+    return v;                                                                  \
+  }
+SHMEM_B200_RMA_TYPES(DEF_RMA)
+
+/* ---- synchronisation ---------------------------------------------------------- */
+static int barrier_on(b200_team_t *t, int algo) {
+  coll_t r = {0};
+  r.kind = K_BARRIER;
+  r.algo = algo;
+  return arrive(t, &r);
+}
+void shmem_barrier_all(void) { barrier_on(&g_world, g_barrier_all_algo); }
+void shmem_sync_all(void) { barrier_on(&g_world, g_sync_all_algo); }
+void shmem_barrier(int PE_start, int logPE_stride, int PE_size, long *pSync) {
+  (void)pSync; /* the engine owns its flag words */
+  barrier_on(active_set(PE_start, logPE_stride, PE_size), g_barrier_algo);
+}
+void shmem_sync(int PE_start, int logPE_stride, int PE_size, long *pSync) {
+  (void)pSync;
+  barrier_on(active_set(PE_start, logPE_stride, PE_size), g_sync_algo);
+}
+int shmem_team_sync(shmem_team_t team) {
+  return barrier_on((b200_team_t *)team, g_team_sync_algo);
+}
+
+/* ---- teams --------------------------------------------------------------------- */
+int shmem_team_my_pe(shmem_team_t team) { return team_index((b200_team_t *)team, t_pe); }
+int shmem_team_n_pes(shmem_team_t team) {
+  b200_team_t *t = (b200_team_t *)team;
+  return (t && t->valid) ? t->size : -1;
+}
+int shmem_team_translate_pe(shmem_team_t src_team, int src_pe, shmem_team_t dest_team) {
+  b200_team_t *s = (b200_team_t *)src_team;
+  if (!s || !s->valid || src_pe < 0 || src_pe >= s->size) return -1;
+  return team_index((b200_team_t *)dest_team, s->start + src_pe * s->stride);
+}
+int shmem_team_get_config(shmem_team_t team, long config_mask, shmem_team_config_t *config) {
+  (void)config_mask;
+  if (!team || !config) return -1;
+  config->num_contexts = 0;
+  return 0;
+}
+int shmem_team_split_strided(shmem_team_t parent_team, int start, int stride, int size,
+                             const shmem_team_config_t *config, long config_mask,
+                             shmem_team_t *new_team) {
+  (void)config;
+  (void)config_mask;
+  b200_team_t *p = (b200_team_t *)parent_team;
+  coll_t r = {0};
+  r.kind = K_SPLIT;
+  r.a = start;
+  r.b = stride;
+  r.n = (uint64_t)size;
+  int rc = arrive(p, &r);
+  if (new_team) *new_team = SHMEM_TEAM_INVALID;
+  if (rc) return -1;
+  b200_team_t *n = (b200_team_t *)p->agg.outp;
+  if (new_team && team_index(n, t_pe) >= 0) *new_team = n;
+  return 0;
+}
+int shmem_team_split_2d(shmem_team_t parent_team, int xrange,
+                        const shmem_team_config_t *xaxis_config, long xaxis_mask,
+                        shmem_team_t *xaxis_team, const shmem_team_config_t *yaxis_config,
+                        long yaxis_mask, shmem_team_t *yaxis_team) {
+  (void)xaxis_config;
+  (void)xaxis_mask;
+  (void)yaxis_config;
+  (void)yaxis_mask;
+  b200_team_t *p = (b200_team_t *)parent_team;
+  coll_t r = {0};
+  r.kind = K_SPLIT2D;
+  r.a = xrange;
+  if (xaxis_team) *xaxis_team = SHMEM_TEAM_INVALID;
+  if (yaxis_team) *yaxis_team = SHMEM_TEAM_INVALID;
+  if (arrive(p, &r)) return -1;
+  const int i = team_index(p, t_pe);
+  b200_team_t **xs = (b200_team_t **)p->agg.outp, **ys = (b200_team_t **)p->agg.outq;
+  if (xaxis_team) *xaxis_team = xs[i / xrange];
+  if (yaxis_team) *yaxis_team = ys[i % xrange];
+  return 0;
+}
+void shmem_team_destroy(shmem_team_t team) {
+  coll_t r = {0};
+  r.kind = K_DESTROY;
+  if (team && team != SHMEM_TEAM_WORLD) arrive((b200_team_t *)team, &r);
+}
+
+/* ---- reductions --------------------------------------------------------------- */
+#define B200_DTYPE_OF(_type)                                                   \
+  _Generic((_type)0, char: B200SHM_I8, signed char: B200SHM_I8,                \
+           unsigned char: B200SHM_U8, short: B200SHM_I16,                      \
+           unsigned short: B200SHM_U16, int: B200SHM_I32,                      \
+           unsigned int: B200SHM_U32, long: B200SHM_I64,                       \
+           unsigned long: B200SHM_U64, long long: B200SHM_I64,                 \
+           unsigned long long: B200SHM_U64, float: B200SHM_F32,                \
+           double: B200SHM_F64, long double: B200SHM_F80,                      \
+           float _Complex: B200SHM_C32, double _Complex: B200SHM_C64)
+
+static int reduce_on(b200_team_t *t, int op, int dtype, int form, void *dest, const void *source,
+                     size_t n) {
+  coll_t r = {0};
+  r.kind = K_REDUCE;
+  r.op = op;
+  r.dtype = dtype;
+  r.algo = g_reduce_algo[form][op];
+  r.n = n;
+  if (sym_off(dest, &r.dest) || sym_off(source, &r.src)) return t_status = B200SHM_ERR_ARG;
+  return arrive(t, &r);
+}
+
+#define DEF_TEAM_REDUCE(_type, _tn, _op, _OP)                                  \
+  int shmem_##_tn##_##_op##_reduce(shmem_team_t team, _type *dest,            \
+                                   const _type *source, size_t nreduce) {     \
+    return reduce_on((b200_team_t *)team, _OP, B200_DTYPE_OF(_type), 0, dest, \
+                     source, nreduce);                                         \
+  }
+#define DEF_TO_ALL(_type, _tn, _op, _OP)                                       \
+  void shmem_##_tn##_##_op##_to_all(_type *dest, const _type *source,         \
+                                    int nreduce, int PE_start,                 \
+                                    int logPE_stride, int PE_size,             \
+                                    _type *pWrk, long *pSync) {                \
+    (void)pWrk;                                                                \
+    (void)pSync;                                                               \
+    reduce_on(active_set(PE_start, logPE_stride, PE_size), _OP,                \
+              B200_DTYPE_OF(_type), 1, dest, source,                           \
+              nreduce > 0 ? (size_t)nreduce : 0);                              \
+  }
+#define R_AND(_t, _n) DEF_TEAM_REDUCE(_t, _n, and, B200SHM_AND)
+#define R_OR(_t, _n) DEF_TEAM_REDUCE(_t, _n, or, B200SHM_OR)
+#define R_XOR(_t, _n) DEF_TEAM_REDUCE(_t, _n, xor, B200SHM_XOR)
+#define R_MIN(_t, _n) DEF_TEAM_REDUCE(_t, _n, min, B200SHM_MIN)
+#define R_MAX(_t, _n) DEF_TEAM_REDUCE(_t, _n, max, B200SHM_MAX)
+#define R_SUM(_t, _n) DEF_TEAM_REDUCE(_t, _n, sum, B200SHM_SUM)
+#define R_PROD(_t, _n) DEF_TEAM_REDUCE(_t, _n, prod, B200SHM_PROD)
+SHMEM_B200_REDUCE_BITWISE_TYPES(R_AND)
+SHMEM_B200_REDUCE_BITWISE_TYPES(R_OR)
+SHMEM_B200_REDUCE_BITWISE_TYPES(R_XOR)
+SHMEM_B200_REDUCE_MINMAX_TYPES(R_MIN)
+SHMEM_B200_REDUCE_MINMAX_TYPES(R_MAX)
+SHMEM_B200_REDUCE_ARITH_TYPES(R_SUM)
+SHMEM_B200_REDUCE_ARITH_TYPES(R_PROD)
+#define A_AND(_t, _n) DEF_TO_ALL(_t, _n, and, B200SHM_AND)
+#define A_OR(_t, _n) DEF_TO_ALL(_t, _n, or, B200SHM_OR)
+#define A_XOR(_t, _n) DEF_TO_ALL(_t, _n, xor, B200SHM_XOR)
+#define A_MIN(_t, _n) DEF_TO_ALL(_t, _n, min, B200SHM_MIN)
+#define A_MAX(_t, _n) DEF_TO_ALL(_t, _n, max, B200SHM_MAX)
+#define A_SUM(_t, _n) DEF_TO_ALL(_t, _n, sum, B200SHM_SUM)
+#define A_PROD(_t, _n) DEF_TO_ALL(_t, _n, prod, B200SHM_PROD)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(A_AND)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(A_OR)
+SHMEM_B200_TO_ALL_BITWISE_TYPES(A_XOR)
+SHMEM_B200_TO_ALL_MINMAX_TYPES(A_MIN)
+SHMEM_B200_TO_ALL_MINMAX_TYPES(A_MAX)
+SHMEM_B200_TO_ALL_ARITH_TYPES(A_SUM)
+SHMEM_B200_TO_ALL_ARITH_TYPES(A_PROD)
+
+/* ---- data movement -------------------------------------------------------------- */
+static int copy_on(b200_team_t *t, int kind, void *dest, const void *source, uint64_t n,
+                   int64_t a, int64_t b, uint64_t esize, int root) {
+  coll_t r = {0};
+  r.kind = kind;
+  r.n = n;
+  r.a = a;
+  r.b = b;
+  r.esize = esize;
+  r.root = root;
+  if (sym_off(dest, &r.dest) || sym_off(source, &r.src)) return t_status = B200SHM_ERR_ARG;
+  return arrive(t, &r);
+}
+
+#define DEF_COPY(_type, _tn)                                                   \
+  int shmem_##_tn##_fcollect(shmem_team_t team, _type *dest,                  \
+                             const _type *source, size_t nelems) {            \
+    return copy_on((b200_team_t *)team, K_FCOLLECT, dest, source,              \
+                   nelems * sizeof(_type), 0, 0, 0, 0);                        \
+  }                                                                            \
+  int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                  \
+                             const _type *source, size_t nelems) {            \
+    return copy_on((b200_team_t *)team, K_ALLTOALL, dest, source,              \
+                   nelems * sizeof(_type), 0, 0, 0, 0);                        \
+  }                                                                            \
+  int shmem_##_tn##_alltoalls(shmem_team_t team, _type *dest,                 \
+                              const _type *source, ptrdiff_t dst,             \
+                              ptrdiff_t sst, size_t nelems) {                 \
+    return copy_on((b200_team_t *)team, K_ALLTOALLS, dest, source, nelems,     \
+                   dst, sst, sizeof(_type), 0);                                \
+  }                                                                            \
+  int shmem_##_tn##_broadcast(shmem_team_t team, _type *dest,                 \
+                              const _type *source, size_t nelems,             \
+                              int PE_root) {                                   \
+    return copy_on((b200_team_t *)team, K_BROADCAST, dest, source,             \
+                   nelems * sizeof(_type), 0, 0, 0, PE_root);                  \
+  }
+SHMEM_B200_RMA_TYPES(DEF_COPY)
+
+int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems) {
+  return copy_on((b200_team_t *)team, K_FCOLLECT, dest, source, nelems, 0, 0, 0, 0);
+}
+int shmem_alltoallmem(shmem_team_t team, void *dest, const void *source, size_t nelems) {
+  return copy_on((b200_team_t *)team, K_ALLTOALL, dest, source, nelems, 0, 0, 0, 0);
+}
+int shmem_alltoallsmem(shmem_team_t team, void *dest, const void *source, ptrdiff_t dst,
+                       ptrdiff_t sst, size_t nelems) {
+  /* one element of nelems bytes per PE pair (alltoalls.c:397-435) */
+  return copy_on((b200_team_t *)team, K_ALLTOALLS, dest, source, 1, dst, sst, nelems, 0);
+}
+int shmem_broadcastmem(shmem_team_t team, void *dest, const void *source, size_t nelems,
+                       int PE_root) {
+  return copy_on((b200_team_t *)team, K_BROADCAST, dest, source, nelems, 0, 0, 0, PE_root);
+}
+
+#define DEF_SIZED(_bits)                                                       \
+  void shmem_fcollect##_bits(void *target, const void *source, size_t nelems, \
+                             int PE_start, int logPE_stride, int PE_size,      \
+                             long *pSync) {                                    \
+    (void)pSync;                                                               \
+    copy_on(active_set(PE_start, logPE_stride, PE_size), K_FCOLLECT, target,   \
+            source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
+  }                                                                            \
+  void shmem_alltoall##_bits(void *target, const void *source, size_t nelems, \
+                             int PE_start, int logPE_stride, int PE_size,      \
+                             long *pSync) {                                    \
+    (void)pSync;                                                               \
+    copy_on(active_set(PE_start, logPE_stride, PE_size), K_ALLTOALL, target,   \
+            source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
+  }                                                                            \
+  void shmem_alltoalls##_bits(void *target, const void *source, ptrdiff_t dst, \
+                              ptrdiff_t sst, size_t nelems, int PE_start,      \
+                              int logPE_stride, int PE_size, long *pSync) {    \
+    (void)pSync;                                                               \
+    copy_on(active_set(PE_start, logPE_stride, PE_size), K_ALLTOALLS, target,  \
+            source, nelems, dst, sst, _bits / 8, 0);                           \
+  }                                                                            \
+  void shmem_broadcast##_bits(void *target, const void *source, size_t nelems, \
+                              int PE_root, int PE_start, int logPE_stride,     \
+                              int PE_size, long *pSync) {                      \
+    (void)pSync;                                                               \
+    copy_on(active_set(PE_start, logPE_stride, PE_size), K_BROADCAST, target,  \
+            source, nelems * (_bits / 8), 0, 0, 0, PE_root);                   \
+  }
+DEF_SIZED(32)
+DEF_SIZED(64)
+
+/* ---- atomics ------------------------------------------------------------------ */
+static void amo(int op, int dtype, const void *dest, int pe, const void *value, const void *cond,
+                void *fetched) {
+  uint64_t off;
+  if (sym_off(dest, &off)) {
+    t_status = B200SHM_ERR_ARG;
+    return;
+  }
+  t_status = engine_err(b200shm_amo(op, dtype, pe, off, value, cond, fetched));
+}
+
+#define DEF_AMO_STD(_type, _tn)                                                \
+  _type shmem_##_tn##_atomic_fetch_add(_type *dest, _type value, int pe) {    \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH_ADD, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  void shmem_##_tn##_atomic_add(_type *dest, _type value, int pe) {           \
+    amo(B200SHM_AMO_ADD, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
+  }                                                                            \
+  _type shmem_##_tn##_atomic_fetch_inc(_type *dest, int pe) {                 \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL,     \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  void shmem_##_tn##_atomic_inc(_type *dest, int pe) {                        \
+    amo(B200SHM_AMO_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL, NULL);    \
+  }                                                                            \
+  _type shmem_##_tn##_atomic_compare_swap(_type *dest, _type cond,            \
+                                          _type value, int pe) {               \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_CSWAP, B200_DTYPE_OF(_type), dest, pe, &value, &cond,      \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch_add(shmem_ctx_t ctx, _type *dest,      \
+                                           _type value, int pe) {              \
+    (void)ctx;                                                                 \
+    return shmem_##_tn##_atomic_fetch_add(dest, value, pe);                    \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_add(shmem_ctx_t ctx, _type *dest, _type value,\
+                                    int pe) {                                  \
+    (void)ctx;                                                                 \
+    shmem_##_tn##_atomic_add(dest, value, pe);                                 \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch_inc(shmem_ctx_t ctx, _type *dest,      \
+                                           int pe) {                           \
+    (void)ctx;                                                                 \
+    return shmem_##_tn##_atomic_fetch_inc(dest, pe);                           \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_inc(shmem_ctx_t ctx, _type *dest, int pe) {   \
+    (void)ctx;                                                                 \
+    shmem_##_tn##_atomic_inc(dest, pe);                                        \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_compare_swap(shmem_ctx_t ctx, _type *dest,   \
+                                              _type cond, _type value,         \
+                                              int pe) {                        \
+    (void)ctx;                                                                 \
+    return shmem_##_tn##_atomic_compare_swap(dest, cond, value, pe);           \
+  }
+#define DEF_AMO_EXT(_type, _tn)                                                \
+  _type shmem_##_tn##_atomic_swap(_type *dest, _type value, int pe) {         \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_SWAP, B200_DTYPE_OF(_type), dest, pe, &value, NULL, &old); \
+    return old;                                                                \
+  }                                                                            \
+  void shmem_##_tn##_atomic_set(_type *dest, _type value, int pe) {           \
+    amo(B200SHM_AMO_SET, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
+  }                                                                            \
+  _type shmem_##_tn##_atomic_fetch(const _type *source, int pe) {             \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH, B200_DTYPE_OF(_type), source, pe, NULL, NULL,       \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_swap(shmem_ctx_t ctx, _type *dest,           \
+                                      _type value, int pe) {                   \
+    (void)ctx;                                                                 \
+    return shmem_##_tn##_atomic_swap(dest, value, pe);                         \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_set(shmem_ctx_t ctx, _type *dest, _type value,\
+                                    int pe) {                                  \
+    (void)ctx;                                                                 \
+    shmem_##_tn##_atomic_set(dest, value, pe);                                 \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch(shmem_ctx_t ctx, const _type *source,  \
+                                       int pe) {                               \
+    (void)ctx;                                                                 \
+    return shmem_##_tn##_atomic_fetch(source, pe);                             \
+  }
+#define DEF_AMO_BIT(_type, _tn)                                                \
+  _type shmem_##_tn##_atomic_fetch_and(_type *dest, _type value, int pe) {    \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH_AND, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  _type shmem_##_tn##_atomic_fetch_or(_type *dest, _type value, int pe) {     \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH_OR, B200_DTYPE_OF(_type), dest, pe, &value, NULL,    \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  _type shmem_##_tn##_atomic_fetch_xor(_type *dest, _type value, int pe) {    \
+    _type old = 0;                                                             \
+    amo(B200SHM_AMO_FETCH_XOR, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
+        &old);                                                                 \
+    return old;                                                                \
+  }                                                                            \
+  void shmem_##_tn##_atomic_and(_type *dest, _type value, int pe) {           \
+    amo(B200SHM_AMO_AND, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
+  }                                                                            \
+  void shmem_##_tn##_atomic_or(_type *dest, _type value, int pe) {            \
+    amo(B200SHM_AMO_OR, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);   \
+  }                                                                            \
+  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe) {           \
+    amo(B200SHM_AMO_XOR, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
+  }
+SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_STD)
+SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_EXT)
+SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_BIT)

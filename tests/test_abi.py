@@ -39,3 +39,20 @@ def test_calls_before_init_fail_with_state_error():
     assert L.b200shm_fcollect(0, 1, 4, 0, 0, 64, None) == -5
     assert L.b200shm_barrier(2, 0, 1, 4, None) == -5
     assert L.b200shm_ptr(0, 0) is None
+
+
+def test_shmem_surface_exports_every_declared_function():
+    """Every function include/shmem.h and include/shmemx.h declare (after
+    macro expansion) is exported by libshmem_b200.so."""
+    import subprocess
+    import __graft_entry__
+    __graft_entry__.build_library()
+    host_lib = os.path.join(ROOT, "osss-ucx_b200", "lib", "libshmem_b200.so")
+    text = subprocess.run(["gcc", "-E", "-P", "-x", "c", "-"], input='#include "shmemx.h"\n',
+                          capture_output=True, text=True, check=True,
+                          cwd=os.path.join(ROOT, "include")).stdout
+    names = set(re.findall(r"\b((?:shmem|shmemx)_[a-z0-9_]+)\s*\(", text))
+    assert len(names) > 600
+    lib = ctypes.CDLL(host_lib)
+    missing = sorted(n for n in names if not hasattr(lib, n))
+    assert not missing, missing[:20]

@@ -1,0 +1,91 @@
+"""The OpenSHMEM surface (include/shmem.h over libshmem_b200.so): a C program
+written like any OpenSHMEM program (tests/c/spmd_parity.c, 8 PEs) must leave
+in every PE exactly what the reference's algorithms leave there."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "osss-ucx_b200", "lib")
+NP, NR, NFC, NFS, NDM, BLK, NAS = 8, 1024, 256, 4096, 512, 96, 5
+
+OUT = np.dtype([("red", np.int32, (NP, NR)), ("fc", np.int64, (NP, NP * NFC)),
+                ("fs", np.float32, (NP, NFS)), ("dm", np.float64, (NP, NDM)),
+                ("toall", np.int32, (NP, NR)), ("team_even", np.int32, (NP, NR)),
+                ("a2a", np.uint8, (NP, NP * BLK)), ("as", np.int64, (NP, NP * NAS * 2)),
+                ("bcast", np.int64, (NP, NFC)), ("amo_final", np.int64),
+                ("amo_fetched", np.int64, (NP, 4)), ("team_info", np.int32, (NP, 4)),
+                ("status", np.int32, (NP,))], align=True)
+
+
+def compile_program(tmp_path):
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_parity")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_parity.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    return exe
+
+
+def test_program_compiles_and_links_against_the_surface(tmp_path):
+    assert os.path.exists(compile_program(tmp_path))
+
+
+def special_doubles(P, N, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1e6, 1e6, (P, N))
+    pick = rng.integers(0, 8, size=(P, N))
+    x[pick == 0] = 0.0
+    x[pick == 1] = -0.0
+    x[pick == 2] = np.nan
+    return x
+
+
+@pytest.mark.gpu
+def test_spmd_program_matches_oracle(tmp_path, rs):
+    exe = compile_program(tmp_path)
+    red, fc = gen.config1_inputs()
+    fs = gen.normal(np.float32, NP, NFS, 5)
+    dm = special_doubles(NP, NDM, 6)
+    a2a = gen.uniform_int(np.uint8, NP, NP * BLK, 7)
+    as_ = gen.uniform_int(np.int64, NP, NP * NAS * 3, 8)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        for a in (red, fc, fs, dm, a2a, as_):
+            f.write(np.ascontiguousarray(a).tobytes())
+    outp = tmp_path / "out.bin"
+    env = dict(os.environ, SHMEM_SYMMETRIC_SIZE="16M")
+    r = subprocess.run([exe, str(inp), str(outp)], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    o = np.fromfile(outp, dtype=OUT)[0]
+    assert (o["status"] == 0).all()
+    assert o["red"].tobytes() == rs.reduce("rec_dbl", "sum", red).tobytes()
+    assert o["fc"].tobytes() == rs.fcollect(fc).tobytes()
+    assert o["fs"].tobytes() == rs.reduce("rec_dbl", "sum", fs).tobytes()
+    assert o["dm"].tobytes() == rs.reduce("rec_dbl", "max", dm).tobytes()
+    assert o["toall"].tobytes() == o["red"].tobytes()
+    even = rs.reduce("rec_dbl", "sum", red[0::2])
+    assert o["team_even"][0::2].tobytes() == even.tobytes()
+    assert (o["team_even"][1::2] == 0).all()
+    assert o["a2a"].tobytes() == rs.alltoall(a2a).tobytes()
+    assert o["as"].tobytes() == rs.alltoalls(as_, np.zeros((NP, NP * NAS * 2), np.int64), 2, 3,
+                                             NAS).tobytes()
+    want_b = np.zeros((NP, NFC), np.int64)
+    assert o["bcast"].tobytes() == rs.broadcast(fc, want_b, 3).tobytes()
+    assert o["amo_final"] == NP * 4
+    assert sorted(o["amo_fetched"].ravel().tolist()) == list(range(NP * 4))
+    assert all(list(row) == sorted(row) for row in o["amo_fetched"].tolist())
+    info = o["team_info"]
+    for pe in range(NP):
+        if pe % 2 == 0:
+            assert info[pe][0] == pe // 2 and info[pe][1] == NP // 2
+        else:
+            assert info[pe][0] == -1 and info[pe][1] == -1
+        assert info[pe][2] == (pe % 4) * 100 + 4
+        assert info[pe][3] == (pe // 4) * 100 + 2
