@@ -208,8 +208,11 @@ def main():
                     help="time only dtype:op:algo (repeatable), e.g. float32:sum:rec_dbl")
     ap.add_argument("--heap-mb", type=int, default=HEAP >> 20, help="heap slice per PE (MiB)")
     ap.add_argument("--nelems", type=int, default=N, help="elements per PE")
-    ap.add_argument("--workload", default="reduce", choices=["reduce", "movement"],
-                    help="reduce (headline) or movement (alltoall/alltoalls/fcollect/AMO)")
+    ap.add_argument("--workload", default="reduce", choices=["reduce", "movement", "batch"],
+                    help="reduce (headline), movement (alltoall/alltoalls/fcollect/AMO) or "
+                         "batch (4096 reductions over 512 teams of 2048 PEs)")
+    ap.add_argument("--batch-tune", default="auto", choices=["auto", "off"],
+                    help="batch workload: autotune lanes/tile per shape class, or heuristic plan")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -225,6 +228,8 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "movement":
         return run_movement(args, world, rank, local)
+    if args.workload == "batch":
+        return run_batch(args, world, rank, local)
     dist = None
     if world > 1:
         import datetime
@@ -446,6 +451,143 @@ def run_movement(args, world, rank, local):
     if rank == 0:
         print(json.dumps(line), flush=True)
 
+
+# ---------------------------------------------------------------------------
+# batching: 4096 reductions over 512 teams of 2048 PEs
+# ---------------------------------------------------------------------------
+INT_OPS = ["and", "or", "xor", "min", "max", "sum", "prod"]
+BATCH_ES = {"int32": 4, "int64": 8, "float32": 4, "float64": 8}
+
+
+def batch_workload(seed=4, PB=2048, NT=512, NR=4096):
+    """512 teams split_strided from 2048 PEs (sizes power-law in [2, 256],
+    p(s) ~ s^-2, strides cycling 1/2/4, packed along the PEs), 4096
+    reductions: team uniform, nelems log-uniform in [16, 2^18], dtype uniform
+    over int32/int64/float32/float64, op uniform over the 7 ops for ints and
+    sum/prod/min/max for floats.  Buffers sit at team-symmetric offsets (the
+    same offset in every member), the largest teams placed first, which
+    keeps the busiest PE's share of the heap smallest."""
+    rng = np.random.default_rng(seed)
+    u = rng.random(NT)
+    sizes = np.clip((1.0 / (0.5 - u * (0.5 - 1 / 256))).astype(int), 2, 256)
+    teams, pos = [], 0
+    for k, sz in enumerate(sizes):
+        stride = [1, 2, 4][k % 3]
+        span = (int(sz) - 1) * stride + 1
+        teams.append((pos % (PB - span + 1), stride, int(sz)))
+        pos += span
+    reds = []
+    for _ in range(NR):
+        t = int(rng.integers(NT))
+        n = int(np.exp(rng.uniform(np.log(16), np.log(2 ** 18))))
+        dt = ["int32", "int64", "float32", "float64"][int(rng.integers(4))]
+        op = (INT_OPS[int(rng.integers(7))] if dt.startswith("int")
+              else ["sum", "prod", "min", "max"][int(rng.integers(4))])
+        reds.append((t, n, dt, op))
+    need = np.zeros(NT, np.int64)
+    for t, n, dt, _ in reds:
+        need[t] += 2 * ((n * BATCH_ES[dt] + 255) // 256 * 256)
+    top = np.zeros(PB, np.int64)
+    base = np.zeros(NT, np.int64)
+    for t in np.argsort(-sizes, kind="stable"):
+        st, sd, sz = teams[t]
+        mem = st + np.arange(sz) * sd
+        base[t] = top[mem].max()
+        top[mem] = base[t] + need[t]
+    cur = base.copy()
+    items = []
+    for t, n, dt, op in reds:
+        nb = (n * BATCH_ES[dt] + 255) // 256 * 256
+        items.append(dict(op=op, dtype=dt, algo="rec_dbl", team=teams[t], src=int(cur[t]),
+                          dest=int(cur[t] + nb), nelems=n))
+        cur[t] += 2 * nb
+    return items, int(top.max()), sizes
+
+
+def run_batch(args, world, rank, local):
+    """The batching configuration: the same 4096 reductions issued as 4096
+    b200shm_reduce calls, and as one planned batch replayed as a CUDA graph.
+    Inputs are generated on the device (b200shm_fill_uniform: ints in
+    [-1000, 1000], floats in [-1, 1], [0.999, 1.001] for PROD)."""
+    import torch
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    PB = 2048
+    items, heap_need, sizes = batch_workload()
+    B.init(PB, heap_need + (2 << 20))
+    region = B.malloc(heap_need)
+    for k, it in enumerate(items):
+        it["src"] += region
+        it["dest"] += region
+        lo, hi = ((-1000, 1000) if it["dtype"].startswith("int") else
+                  (0.999, 1.001) if it["op"] == "prod" else (-1.0, 1.0))
+        B.fill_uniform(it["src"], it["dtype"], it["nelems"], 1000 + k, lo, hi, team=it["team"])
+    B.quiet()
+    s_ptr = B.stream()
+    st = torch.cuda.ExternalStream(s_ptr)
+    total_bytes = sum(2 * it["team"][2] * it["nelems"] * BATCH_ES[it["dtype"]] for it in items)
+    sample = list(range(0, len(items), 64))
+
+    def snap():
+        return [B.get_rows(items[k]["dest"], items[k]["nelems"] * BATCH_ES[items[k]["dtype"]],
+                           np.uint8, team=items[k]["team"]).tobytes() for k in sample]
+
+    def per_call():
+        for it in items:
+            B.reduce(it["op"], it["dtype"], it["algo"], it["dest"], it["src"], it["nelems"],
+                     team=it["team"], stream=s_ptr)
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        B.quiet()
+        return e0.elapsed_time(e1) / reps
+
+    per_call()
+    B.quiet()
+    want = snap()
+    pc_ms = timed(per_call, max(1, min(args.steps, 5)))
+    flags = B.BATCH_GRAPH | (B.BATCH_NO_TUNE if args.batch_tune == "off" else 0)
+    t0 = time.perf_counter()
+    descs = B.make_descs(items)
+    batch = B.Batch(descs, flags)
+    plan_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        batch.run(s_ptr)
+    B.quiet()
+    launches0 = B.launch_count()
+    b_ms = timed(lambda: batch.run(s_ptr), args.steps)
+    launches = (B.launch_count() - launches0) / args.steps
+    match = snap() == want
+    peak, peak_kind = peaks()
+    line = {"metric": METRIC, "workload": "batch", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup,
+            "config": {"npes": PB, "teams": 512, "team_size_alpha": 2,
+                       "team_size_mean": round(float(sizes.mean()), 2),
+                       "team_size_max": int(sizes.max()), "reductions": len(items),
+                       "nelems": "log-uniform [16, 2^18]", "dtypes": "int32/int64/float32/float64",
+                       "ops": "7 ops on ints, sum/prod/min/max on floats", "algo": "rec_dbl",
+                       "heap_per_pe_bytes": heap_need + (2 << 20)},
+            "batched": {"ms": round(b_ms, 4), "ops_per_s": round(len(items) / (b_ms / 1e3), 1),
+                        "gbs": round(total_bytes / (b_ms / 1e3) / 1e9, 1),
+                        "frac_of_hbm": round(total_bytes / (b_ms / 1e3) / 1e9 / peak, 4),
+                        "form": "CUDA graph: one persistent kernel per (type, op, order) group "
+                                "on 4 side streams + MIN/MAX replay",
+                        "plan_seconds": round(plan_s, 2), "autotune": args.batch_tune,
+                        "lanes_histogram": np.bincount([d.lanes for d in descs],
+                                                       minlength=9).tolist()},
+            "per_call": {"ms": round(pc_ms, 4), "ops_per_s": round(len(items) / (pc_ms / 1e3), 1),
+                         "gbs": round(total_bytes / (pc_ms / 1e3) / 1e9, 1),
+                         "form": "4096 b200shm_reduce calls, stream-ordered"},
+            "speedup": round(pc_ms / b_ms, 2), "alg_bytes": total_bytes,
+            "hbm_floor_ms": round(total_bytes / (peak * 1e9) * 1e3, 4), "peak_kind": peak_kind,
+            "batch_matches_per_call": bool(match), "gpu_launches_per_batch": launches}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -163,6 +163,62 @@ int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size,
                     void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* batched reductions                                                      */
+/* ---------------------------------------------------------------------- */
+
+/* algo value that lets the library choose (rec_dbl, the reference's
+ * default, src/shcoll/src/defaults.h:71) */
+#define B200SHM_ALGO_AUTO (-1)
+
+/* One reduction of a batch: the arguments of b200shm_reduce.  `lanes` and
+ * `tile` are outputs of b200shm_batch_create: the lanes per 16-byte column
+ * and the units per tile the autotuner chose (0 = this reduction runs as
+ * its own launch because the batch kernels do not cover its
+ * (dtype, op, algo, size)); `algo` is rewritten when it was AUTO. */
+typedef struct b200shm_reduce_desc {
+  int32_t op, dtype, algo;
+  int32_t pe_start, pe_stride, pe_size;
+  uint64_t dest_off, src_off, nelems;
+  int32_t lanes, tile;
+} b200shm_reduce_desc;
+
+typedef struct b200shm_batch b200shm_batch;
+
+#define B200SHM_BATCH_NO_TUNE 0x1 /* heuristic plan, no timing runs        */
+#define B200SHM_BATCH_GRAPH 0x2   /* capture the run into a CUDA graph     */
+
+/* Plan a batch of n independent reductions: validate every descriptor,
+ * let the autotuner choose lanes and tile per shape class (timing
+ * candidates on the device the first time a class is seen; the choice is
+ * cached for the process), and upload the plan.  The reductions run
+ * concurrently, so a descriptor whose dest touches another descriptor's
+ * source or dest (in any member) is rejected with B200SHM_ERR_ARG; sharing
+ * a source, and a descriptor in place, are fine.  Replaces n separate
+ * shcoll_<T>_<op>_reduce_<algo> calls (src/shcoll/src/reduce.c:1078-1102),
+ * which the reference can only issue one after the other.  Every result is
+ * bit-identical to b200shm_reduce on the same descriptor. */
+int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
+                         b200shm_batch **out);
+/* Run the whole batch: one persistent launch per (type, op, combine order)
+ * group, the groups overlapping on side streams, plus one launch that
+ * replays order-dependent float MIN/MAX elements and one launch per
+ * reduction the batch kernels do not cover.  With B200SHM_BATCH_GRAPH the
+ * run is a single CUDA graph launch.  Runs of one batch must not overlap
+ * on the GPU (they share its tile counters). */
+int b200shm_batch_run(b200shm_batch *batch, void *stream);
+int b200shm_batch_destroy(b200shm_batch *batch);
+/* create + run + destroy. */
+int b200shm_reduce_batch(b200shm_reduce_desc *descs, uint64_t n, void *stream);
+
+/* Fill nelems elements of `dtype` at `off` in pe_count members with seeded
+ * pseudo-random values: integers uniform in [lo, hi], floats uniform in
+ * [lo, hi) (the value depends only on seed, global PE and index).  Input
+ * generation on the device for tests and benchmarks. */
+int b200shm_fill_uniform(int pe_start, int pe_stride, int pe_count, uint64_t off,
+                         int dtype, uint64_t nelems, uint64_t seed, double lo,
+                         double hi, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* atomics                                                                 */
 /* ---------------------------------------------------------------------- */
 

@@ -68,6 +68,12 @@ def _load():
         "b200shm_broadcast": (ci, [ci, ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_barrier": (ci, [ci, ci, ci, ci, vp]),
         "b200shm_amo_batch": (ci, [ci, ci, u64, vp, vp, vp, vp, vp, vp]),
+        "b200shm_batch_create": (ci, [vp, u64, ci, ctypes.POINTER(vp)]),
+        "b200shm_batch_run": (ci, [vp, vp]),
+        "b200shm_batch_destroy": (ci, [vp]),
+        "b200shm_reduce_batch": (ci, [vp, u64, vp]),
+        "b200shm_fill_uniform": (ci, [ci, ci, ci, u64, ci, u64, u64, ctypes.c_double,
+                                      ctypes.c_double, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -205,3 +211,62 @@ def amo_batch(amo, dtype, nops, pe_dev, off_dev, value_dev=None, cond_dev=None,
     """Device-array AMO batch; *_dev are device addresses (ints)."""
     return _check(lib.b200shm_amo_batch(AMOS.index(amo), DTYPES.index(dtype), nops, pe_dev,
                                         off_dev, value_dev, cond_dev, fetched_dev, stream))
+
+
+# ---------------------------------------------------------------------------
+# batched reductions
+# ---------------------------------------------------------------------------
+BATCH_NO_TUNE = 0x1
+BATCH_GRAPH = 0x2
+
+
+class ReduceDesc(ctypes.Structure):
+    """b200shm_reduce_desc"""
+    _fields_ = [("op", ctypes.c_int32), ("dtype", ctypes.c_int32), ("algo", ctypes.c_int32),
+                ("pe_start", ctypes.c_int32), ("pe_stride", ctypes.c_int32),
+                ("pe_size", ctypes.c_int32), ("dest_off", ctypes.c_uint64),
+                ("src_off", ctypes.c_uint64), ("nelems", ctypes.c_uint64),
+                ("lanes", ctypes.c_int32), ("tile", ctypes.c_int32)]
+
+
+def make_descs(items):
+    """items: dicts with op, dtype, algo ("auto" allowed), team=(start, stride, size),
+    dest, src, nelems."""
+    arr = (ReduceDesc * len(items))()
+    for i, it in enumerate(items):
+        start, stride, size = it["team"]
+        algo = it.get("algo", "rec_dbl")
+        arr[i] = ReduceDesc(OPS.index(it["op"]), DTYPES.index(it["dtype"]),
+                            -1 if algo == "auto" else ALGOS.index(algo), start, stride, size,
+                            it["dest"], it["src"], it["nelems"], 0, 0)
+    return arr
+
+
+class Batch:
+    """A planned batch of independent reductions (b200shm_batch_create / run / destroy)."""
+
+    def __init__(self, descs, flags=0):
+        self.descs = descs
+        self.h = None
+        h = ctypes.c_void_p()
+        _check(lib.b200shm_batch_create(ctypes.cast(descs, ctypes.c_void_p), len(descs), flags,
+                                        ctypes.byref(h)))
+        self.h = h
+
+    def run(self, stream=None):
+        return _check(lib.b200shm_batch_run(self.h, stream))
+
+    def close(self):
+        if self.h:
+            lib.b200shm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def fill_uniform(off, dtype, nelems, seed, lo, hi, team=None, stream=None):
+    """Seeded uniform values at `off` in every member (ints in [lo, hi], floats in [lo, hi))."""
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_fill_uniform(start, stride, size, off, DTYPES.index(dtype), nelems,
+                                           seed, lo, hi, stream))

@@ -58,8 +58,13 @@ int cuda_fail(cudaError_t e, const char *what);
     if (_e != cudaSuccess) return ::b200::cuda_fail(_e, #call);                \
   } while (0)
 
+/* bytes per element of each b200shm_dtype (long double occupies 16) */
+static constexpr int kDtypeSize[B200SHM_NDTYPE] = {1, 2, 4, 8, 1, 2, 4, 8, 4, 8, 16, 8, 16};
+
 /* Kernels launched by this library since load (b200shm_launch_count). */
 void count_launch(unsigned n = 1);
+/* launches recorded into a CUDA graph run only when it is replayed */
+void uncount_launches(unsigned long long n);
 
 /* Resolve the stream argument of an entry point. */
 inline cudaStream_t pick_stream(void *s) {
@@ -86,6 +91,10 @@ inline unsigned grid_for(uint64_t items, int threads, int per_sm) {
   if (need < 1) need = 1;
   return (unsigned)(need < cap ? need : cap);
 }
+
+/* The per-call reduce (reduce.cu), validated and enqueued on stream s. */
+int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
+                  uint64_t dest_off, uint64_t src_off, uint64_t nelems, cudaStream_t s);
 
 /* Member addressing: member i of a team lives at
  * base + (pe_start + i*pe_stride) * slice + off. */

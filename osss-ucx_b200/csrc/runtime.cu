@@ -28,6 +28,7 @@ State &st() { return g_state; }
 static thread_local char t_err[512] = "";
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 
 int fail(int code, const char *fmt, ...) {
   va_list ap;
