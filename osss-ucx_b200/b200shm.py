@@ -257,9 +257,9 @@ class Batch:
         return _check(lib.b200shm_batch_run(self.h, stream))
 
     def close(self):
-        if self.h:
+        if self.h and lib is not None:  # lib is None during interpreter teardown
             lib.b200shm_batch_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()

@@ -142,47 +142,66 @@ __device__ void run_tile(const BDesc &d, uint32_t di, uint64_t u0, uint64_t cnt,
             }
         }
       } else {
-        /* The lane's members are loaded 8 at a time (extras included, so
-         * no load waits on another) and fed in member order through a
-         * binary counter over the lane's leaves: pushing leaf c combines
-         * it with the complete subtrees of the levels below ffs(~c) - 1,
-         * which is the reference tree's shape. */
-        PK y;
+        /* The lane's leaves are taken KB at a time: their own members and
+         * (for a butterfly over a non-power-of-two team) extra members
+         * are all loaded before any is used, the extras are folded on
+         * (op(extra, own)), a full batch is reduced as a register subtree
+         * of KB leaves, and subtrees enter a binary counter kept in shared
+         * memory: pushing a subtree of 2^lv leaves when c leaves are in
+         * combines it with the stacked subtrees of levels lv .. lv +
+         * (trailing ones of c >> lv) - 1, earlier subtree first -- the
+         * reference tree's shape.  8 leaves without extras, 4 with: either
+         * way at most 8 loads, and registers for 8 packs, in flight. */
         int c = 0;
-        int own = m0, nxt = member_of(l0 + 1);
-        auto push = [&](PK v) {
-          const int t = __ffs(~c) - 1;
-          for (int L = 0; L < t; L++) v = comb(stk_get<PK>(stk, L), v);
+        auto push_lv = [&](PK v, int lv) {
+          const int t = __ffs(~(c >> lv)) - 1 + lv;
+          for (int L = lv; L < t; L++) v = comb(stk_get<PK>(stk, L), v);
           stk_put(stk, t, v);
-          c++;
+          c += 1 << lv;
         };
-        for (int mb = m0; mb < m1; mb += 8) {
-          PK x[8];
+        auto leaves = [&](auto kb_c, auto ex_c) {
+          constexpr int KB = decltype(kb_c)::value;
+          constexpr bool EX = decltype(ex_c)::value;
+          constexpr int LB = KB == 8 ? 3 : 2;
+          for (int qb = l0; qb < l1; qb += KB) {
+            const int k = l1 - qb < KB ? l1 - qb : KB;
+            PK x[KB], e[EX ? KB : 1];
+            bool ex[KB];
 #pragma unroll
-          for (int u = 0; u < 8; u++)
-            if (mb + u < m1) x[u] = ld_pack<T, V>(src + (uint64_t)(mb + u) * d.step);
-#pragma unroll
-          for (int u = 0; u < 8; u++)
-            if (mb + u < m1) {
-              if constexpr (ORDER == ORD_BUTTERFLY) {
-                const int m = mb + u;
-                if (m == own) { /* a leaf's own member; its extra may follow */
-                  y = x[u];
-                  if (nxt == m + 1) {
-                    push(y);
-                    own = nxt;
-                    nxt = member_of(l0 + c + 1);
-                  }
-                } else { /* the extra member folds onto its leaf: op(extra, own) */
-                  push(papply<OP>(x[u], y));
-                  own = nxt;
-                  nxt = member_of(l0 + c + 1);
+            for (int u = 0; u < KB; u++) {
+              ex[u] = false;
+              if (u < k) {
+                const int mo = member_of(qb + u);
+                x[u] = ld_pack<T, V>(src + (uint64_t)mo * d.step);
+                if constexpr (EX) {
+                  ex[u] = member_of(qb + u + 1) - mo == 2;
+                  if (ex[u]) e[u] = ld_pack<T, V>(src + (uint64_t)(mo + 1) * d.step);
                 }
-              } else {
-                push(x[u]);
               }
             }
-        }
+            if constexpr (EX) {
+#pragma unroll
+              for (int u = 0; u < KB; u++)
+                if (ex[u]) x[u] = papply<OP>(e[u], x[u]);
+            }
+            if (k == KB) {
+#pragma unroll
+              for (int w = KB; w > 1; w >>= 1) {
+#pragma unroll
+                for (int i = 0; i < w / 2; i++) x[i] = comb(x[2 * i], x[2 * i + 1]);
+              }
+              push_lv(x[0], LB);
+            } else {
+#pragma unroll
+              for (int u = 0; u < KB; u++)
+                if (u < k) push_lv(x[u], 0);
+            }
+          }
+        };
+        if (ORDER == ORD_BUTTERFLY && P != d.p2s)
+          leaves(std::integral_constant<int, 4>{}, std::true_type{});
+        else
+          leaves(std::integral_constant<int, 8>{}, std::false_type{});
         const int n = l1 - l0;
         if ((n & (n - 1)) == 0) {
           r = stk_get<PK>(stk, __ffs(n) - 1);
@@ -253,7 +272,7 @@ __device__ __forceinline__ void run_desc_tile(const BDesc &d, uint32_t di, uint3
 /* One (type, op, order) group of a batch: descriptors [d0, d0+nd) of the
  * plan (sorted by group), tiles taken from the group's counter. */
 template <class T, int OP, int ORDER, bool MM>
-__global__ void __launch_bounds__(kBatchThreads) k_batch_group(const BPlan p, uint32_t d0,
+__global__ void __launch_bounds__(kBatchThreads, 2) k_batch_group(const BPlan p, uint32_t d0,
                                                                uint32_t nd, unsigned *counter) {
   __shared__ unsigned s_tile;
   /* 16-byte packs: 4 words per level per thread (chains keep no stack) */

@@ -117,10 +117,27 @@ struct alignas(V * sizeof(T) >= 16 ? 16 : alignof(T)) Pack {
   T x[V];
 };
 
+/* 16-byte packs move with one vector access whose registers have the
+ * element's own class (f64 pairs, u64, f32, u32), so no moves are needed
+ * between the load and the arithmetic. */
 template <class T, int V>
 __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
   Pack<T, V> r;
-  if constexpr (sizeof(Pack<T, V>) == 16) {
+  if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];"
+        : "=d"(r.x[0]), "=d"(r.x[1])
+        : "l"(p));
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_integral<T>::value &&
+                       sizeof(T) == 8) {
+    unsigned long long a, b;
+    asm("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+    r.x[0] = (T)a;
+    r.x[1] = (T)b;
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, float>::value) {
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+        : "=f"(r.x[0]), "=f"(r.x[1]), "=f"(r.x[2]), "=f"(r.x[3])
+        : "l"(p));
+  } else if constexpr (sizeof(Pack<T, V>) == 16) {
     uint4 u;
     asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
         : "=r"(u.x), "=r"(u.y), "=r"(u.z), "=r"(u.w)
@@ -133,7 +150,19 @@ __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
 }
 template <class T, int V>
 __device__ __forceinline__ void st_pack(char *p, const Pack<T, V> &v) {
-  if constexpr (sizeof(Pack<T, V>) == 16) {
+  if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
+    asm volatile("st.global.v2.f64 [%0], {%1,%2};" ::"l"(p), "d"(v.x[0]), "d"(v.x[1])
+                 : "memory");
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_integral<T>::value &&
+                       sizeof(T) == 8) {
+    asm volatile("st.global.v2.u64 [%0], {%1,%2};" ::"l"(p),
+                 "l"((unsigned long long)v.x[0]), "l"((unsigned long long)v.x[1])
+                 : "memory");
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, float>::value) {
+    asm volatile("st.global.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(v.x[0]), "f"(v.x[1]),
+                 "f"(v.x[2]), "f"(v.x[3])
+                 : "memory");
+  } else if constexpr (sizeof(Pack<T, V>) == 16) {
     uint4 u;
     memcpy(&u, &v, 16);
     asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y),
