@@ -210,6 +210,74 @@ int b200shm_batch_destroy(b200shm_batch *batch);
 /* create + run + destroy. */
 int b200shm_reduce_batch(b200shm_reduce_desc *descs, uint64_t n, void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* serving loop                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* Request kinds of the serving loop. */
+enum b200shm_req_kind {
+  B200SHM_REQ_REDUCE = 0, /* all-reduce over the team, as b200shm_reduce      */
+  B200SHM_REQ_FCOLLECT,   /* as b200shm_fcollect, n = bytes per member        */
+  B200SHM_REQ_ALLTOALL,   /* as b200shm_alltoall, n = bytes per block         */
+  B200SHM_REQ_PUT,        /* n bytes from PE pe_start's src_off to PE pe's dest_off */
+  B200SHM_REQ_GET,        /* n bytes from PE pe's src_off to PE pe_start's dest_off */
+  B200SHM_REQ_AMO,        /* op = b200shm_amo on (pe, dest_off), as b200shm_amo */
+  B200SHM_REQ_NKIND
+};
+
+/* One request.  REDUCE: op/dtype/algo/team/dest/src/n = nelems, as
+ * b200shm_reduce (dtype one of I32, U32, I64, U64, F32, F64).  AMO: op is
+ * a b200shm_amo, dtype a 4- or 8-byte type, value/cond hold the operand
+ * bits, the old value comes back through b200shm_serve_poll. */
+typedef struct b200shm_request {
+  int32_t kind, op, dtype, algo;
+  int32_t pe_start, pe_stride, pe_size, pe;
+  uint64_t dest_off, src_off, n;
+  uint64_t value, cond;
+} b200shm_request;
+
+typedef struct b200shm_server b200shm_server;
+
+/* Start the serving loop: a persistent kernel of `ctas` CTAs (0 = one per
+ * SM) on its own stream that drains a ring of queue_slots requests kept in
+ * mapped host memory.  Requests are cut into tiles that idle CTAs claim,
+ * so a large request spreads over the GPU while small ones pass it; each
+ * request reports completion through a word in host memory.  A CTA with no
+ * published work for idle_seconds (0 = 1 s) exits; the host relaunches the
+ * kernel when new work arrives, so the loop holds the GPU only while it is
+ * used.  Replaces the reference's issue-one-call-and-wait model
+ * (shmem_* -> shcoll / shmemc_ctx_* round trips, src/shcoll/src/*.c,
+ * src/shmemc/ucx/comms.c) for streams of small operations.  Requests in
+ * flight together may run in any order and concurrently, as non-blocking
+ * (_nbi) operations do: a request that depends on another's result must
+ * be enqueued after that one completed.  While a server runs, calls that
+ * synchronise the whole device (cudaDeviceSynchronize, cudaFree) wait for
+ * it to go idle. */
+int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
+                        b200shm_server **out);
+/* Validate and publish one request; *ticket identifies it.  Returns
+ * B200SHM_ERR_BUSY when all queue slots hold requests not yet complete. */
+int b200shm_serve_enqueue(b200shm_server *srv, const b200shm_request *req,
+                          uint64_t *ticket);
+/* 1 when the request completed (its AMO old value in *fetched, which may
+ * be NULL), 0 while it is pending, < 0 on an error. */
+int b200shm_serve_poll(b200shm_server *srv, uint64_t ticket, uint64_t *fetched);
+/* Block until the request completes or timeout_seconds pass
+ * (B200SHM_ERR_TIMEOUT). */
+int b200shm_serve_wait(b200shm_server *srv, uint64_t ticket, double timeout_seconds,
+                       uint64_t *fetched);
+/* Let the loop drain, wait (bounded) for its kernel to exit, free it. */
+int b200shm_serve_stop(b200shm_server *srv);
+/* Open-loop replay of n requests: request k is issued at arrival_s[k]
+ * seconds after the call starts (through the server when srv is non-NULL,
+ * else as one blocking per-call entry point each: b200shm_reduce,
+ * _fcollect, _alltoall, _memcpy, _amo), and latency_s[k] receives the time
+ * from its arrival to the observed completion.  fetched (may be NULL)
+ * receives AMO old values.  The measuring tool behind the serving
+ * benchmark and its per-call comparison. */
+int b200shm_serve_replay(b200shm_server *srv, const b200shm_request *reqs, uint64_t n,
+                         const double *arrival_s, double *latency_s, uint64_t *fetched);
+
 /* Fill nelems elements of `dtype` at `off` in pe_count members with seeded
  * pseudo-random values: integers uniform in [lo, hi], floats uniform in
  * [lo, hi) (the value depends only on seed, global PE and index).  Input

@@ -74,6 +74,13 @@ def _load():
         "b200shm_reduce_batch": (ci, [vp, u64, vp]),
         "b200shm_fill_uniform": (ci, [ci, ci, ci, u64, ci, u64, u64, ctypes.c_double,
                                       ctypes.c_double, vp]),
+        "b200shm_serve_start": (ci, [ctypes.c_uint32, ci, ctypes.c_double, ctypes.POINTER(vp)]),
+        "b200shm_serve_enqueue": (ci, [vp, vp, ctypes.POINTER(u64)]),
+        "b200shm_serve_poll": (ci, [vp, u64, ctypes.POINTER(u64)]),
+        "b200shm_serve_wait": (ci, [vp, u64, ctypes.c_double, ctypes.POINTER(u64)]),
+        "b200shm_serve_stop": (ci, [vp]),
+        "b200shm_serve_replay": (ci, [vp, vp, u64, vp, vp, vp]),
+        "b200shm_amo": (ci, [ci, ci, ci, u64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -270,3 +277,89 @@ def fill_uniform(off, dtype, nelems, seed, lo, hi, team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_fill_uniform(start, stride, size, off, DTYPES.index(dtype), nelems,
                                            seed, lo, hi, stream))
+
+
+# ---------------------------------------------------------------------------
+# serving loop
+# ---------------------------------------------------------------------------
+REQ_KINDS = ["reduce", "fcollect", "alltoall", "put", "get", "amo"]
+
+
+class Request(ctypes.Structure):
+    """b200shm_request"""
+    _fields_ = [("kind", ctypes.c_int32), ("op", ctypes.c_int32), ("dtype", ctypes.c_int32),
+                ("algo", ctypes.c_int32), ("pe_start", ctypes.c_int32),
+                ("pe_stride", ctypes.c_int32), ("pe_size", ctypes.c_int32),
+                ("pe", ctypes.c_int32), ("dest_off", ctypes.c_uint64),
+                ("src_off", ctypes.c_uint64), ("n", ctypes.c_uint64),
+                ("value", ctypes.c_uint64), ("cond", ctypes.c_uint64)]
+
+
+def make_requests(items):
+    """items: dicts with kind and the fields it uses: op (a reduce op name, or
+    an AMO name for kind "amo"), dtype, algo, team=(start, stride, size),
+    pe, dest, src, n, value, cond."""
+    arr = (Request * len(items))()
+    for i, it in enumerate(items):
+        kind = it["kind"]
+        start, stride, size = it.get("team", (0, 1, 1))
+        op = it.get("op", "sum")
+        opi = AMOS.index(op) if kind == "amo" else OPS.index(op)
+        algo = it.get("algo", "rec_dbl")
+        arr[i] = Request(REQ_KINDS.index(kind), opi, DTYPES.index(it.get("dtype", "int64")),
+                         -1 if algo == "auto" else ALGOS.index(algo), start, stride, size,
+                         it.get("pe", 0), it.get("dest", 0), it.get("src", 0), it.get("n", 0),
+                         it.get("value", 0) & (2 ** 64 - 1), it.get("cond", 0) & (2 ** 64 - 1))
+    return arr
+
+
+class Server:
+    """The serving loop (b200shm_serve_start / enqueue / poll / wait / stop)."""
+
+    def __init__(self, queue_slots=1024, ctas=0, idle_seconds=1.0):
+        h = ctypes.c_void_p()
+        _check(lib.b200shm_serve_start(queue_slots, ctas, idle_seconds, ctypes.byref(h)))
+        self.h = h
+
+    def enqueue(self, req):
+        t = ctypes.c_uint64()
+        _check(lib.b200shm_serve_enqueue(self.h, ctypes.byref(req), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        f = ctypes.c_uint64()
+        rc = lib.b200shm_serve_poll(self.h, ticket, ctypes.byref(f))
+        if rc < 0:
+            _check(rc)
+        return (rc == 1), f.value
+
+    def wait(self, ticket, timeout=30.0):
+        f = ctypes.c_uint64()
+        _check(lib.b200shm_serve_wait(self.h, ticket, timeout, ctypes.byref(f)))
+        return f.value
+
+    def replay(self, reqs, arrival_s):
+        return replay(reqs, arrival_s, self)
+
+    def stop(self):
+        if self.h and lib is not None:
+            _check(lib.b200shm_serve_stop(self.h))
+        self.h = None
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                self.stop()
+            except Exception:
+                pass
+
+
+def replay(reqs, arrival_s, server=None):
+    """Open-loop replay: returns (latency seconds per request, fetched values)."""
+    n = len(reqs)
+    arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+    lat = np.zeros(n, np.float64)
+    fet = np.zeros(n, np.uint64)
+    _check(lib.b200shm_serve_replay(server.h if server else None, ctypes.cast(reqs, ctypes.c_void_p),
+                                    n, arr.ctypes.data, lat.ctypes.data, fet.ctypes.data))
+    return lat, fet
