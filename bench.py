@@ -208,9 +208,15 @@ def main():
                     help="time only dtype:op:algo (repeatable), e.g. float32:sum:rec_dbl")
     ap.add_argument("--heap-mb", type=int, default=HEAP >> 20, help="heap slice per PE (MiB)")
     ap.add_argument("--nelems", type=int, default=N, help="elements per PE")
-    ap.add_argument("--workload", default="reduce", choices=["reduce", "movement", "batch"],
-                    help="reduce (headline), movement (alltoall/alltoalls/fcollect/AMO) or "
-                         "batch (4096 reductions over 512 teams of 2048 PEs)")
+    ap.add_argument("--workload", default="reduce",
+                    choices=["reduce", "movement", "batch", "serve"],
+                    help="reduce (headline), movement (alltoall/alltoalls/fcollect/AMO), "
+                         "batch (4096 reductions over 512 teams of 2048 PEs) or serve "
+                         "(open-loop request stream over 256 PEs)")
+    ap.add_argument("--serve-requests", type=int, default=100000)
+    ap.add_argument("--serve-rate", type=float, default=200000.0, help="arrivals per second")
+    ap.add_argument("--serve-percall", type=int, default=20000,
+                    help="requests replayed through the per-call entry points")
     ap.add_argument("--batch-tune", default="auto", choices=["auto", "off"],
                     help="batch workload: autotune lanes/tile per shape class, or heuristic plan")
     args = ap.parse_args()
@@ -230,6 +236,8 @@ def main():
         return run_movement(args, world, rank, local)
     if args.workload == "batch":
         return run_batch(args, world, rank, local)
+    if args.workload == "serve":
+        return run_serve(args, world, rank, local)
     dist = None
     if world > 1:
         import datetime
@@ -586,6 +594,152 @@ def run_batch(args, world, rank, local):
             "speedup": round(pc_ms / b_ms, 2), "alg_bytes": total_bytes,
             "hbm_floor_ms": round(total_bytes / (peak * 1e9) * 1e3, 4), "peak_kind": peak_kind,
             "batch_matches_per_call": bool(match), "gpu_launches_per_batch": launches}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# serving: an open-loop request stream over 256 PEs
+# ---------------------------------------------------------------------------
+SERVE_KINDS = ["reduce", "fcollect", "alltoall", "put", "get", "amo"]
+
+
+def serve_workload(nreq, rate, seed=6, PS=256, slice_bytes=256 << 20, slots=256):
+    """nreq requests with Poisson arrivals at `rate`/s: kind uniform over
+    reduce/fcollect/alltoall/put/get/atomic, payload (bytes each PE
+    receives) log-uniform in [8 B, 4 MiB], dtype uniform over
+    int32/int64/float32/float64, team uniform over 64 teams of 4 PEs
+    (PEs 4k..4k+3); reduce algorithm rec_dbl; atomics are int64 fetch-adds of
+    1 on 4096 counters per PE.  Sources are read from two 16 MiB regions per
+    PE (float32 and float64 values uniform in [-1, 1]); every request gets
+    its own dest at team-symmetric offsets of a ring that no two of any
+    `slots` consecutive requests share."""
+    rng = np.random.default_rng(seed)
+    SRC, NCTR = 16 << 20, 4096
+    src32, src64, ctr = 0, SRC, 2 * SRC
+    ring0 = (ctr + NCTR * 8 + 4095) // 4096 * 4096
+    ring_bytes = slice_bytes - ring0 - (2 << 20)
+    arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    arrival -= arrival[0]
+    payload = np.exp(rng.uniform(np.log(8), np.log(4 << 20), nreq)).astype(np.int64)
+    items, needs = [], []
+    pos = 0
+    for k in range(nreq):
+        kind = SERVE_KINDS[int(rng.integers(6))]
+        t = int(rng.integers(64))
+        team = (4 * t, 1, 4)
+        pl = int(payload[k])
+        if kind == "amo":
+            items.append(dict(kind="amo", op="fetch_add", dtype="int64", pe=int(rng.integers(PS)),
+                              dest=ctr + 8 * int(rng.integers(NCTR)), value=1, bytes=8))
+            continue
+        dt = ["int32", "int64", "float32", "float64"][int(rng.integers(4))]
+        es = 4 if dt.endswith("32") else 8
+        region = src32 if es == 4 else src64
+        ne = max(1, pl // es)  # payload in whole elements of the dtype
+        if kind == "reduce":
+            n = ne
+            nb, sb = n * es, n * es
+        elif kind in ("fcollect", "alltoall"):
+            n = max(1, ne // 4) * es
+            nb, sb = 4 * n, (n if kind == "fcollect" else 4 * n)
+        else:
+            n = ne * es
+            nb, sb = n, n
+        so = region + int(rng.integers(0, (SRC - sb) // 16 + 1)) * 16
+        need = (nb + 255) // 256 * 256
+        if pos + need > ring_bytes:
+            pos = 0
+        d = ring0 + pos
+        pos += need
+        needs.append(need)
+        it = dict(kind=kind, team=team, src=so, dest=d, n=n, bytes=nb)
+        if kind == "reduce":
+            op = (INT_OPS[int(rng.integers(7))] if dt.startswith("int")
+                  else ["sum", "prod", "min", "max"][int(rng.integers(4))])
+            it.update(op=op, dtype=dt, algo="rec_dbl")
+        elif kind in ("put", "get"):
+            it.update(team=(4 * t + int(rng.integers(4)), 1, 1), pe=int(rng.integers(PS)))
+        items.append(it)
+    # no two of any `slots` consecutive ring users share a byte: a window's
+    # needs (plus at most one wrap's waste, < 4 MiB) stay under one lap
+    c = np.concatenate([[0], np.cumsum(needs)])
+    w = min(slots, len(needs))
+    assert len(needs) == 0 or (c[w:] - c[:-w]).max() <= ring_bytes - (8 << 20), "ring too small"
+    return items, arrival
+
+
+def run_serve(args, world, rank, local):
+    """The serving configuration: the open-loop stream through the serving
+    loop (latency from each request's arrival to its observed completion
+    word), the same stream saturating (all arrivals at 0), and the per-call
+    entry points (one blocking call per request, in arrival order) on the
+    first --serve-percall requests of the stream."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    PS, SL, SLOTS = 256, 256 << 20, 256
+    items, arrival = serve_workload(args.serve_requests, args.serve_rate, PS=PS, slice_bytes=SL,
+                                    slots=SLOTS)
+    B.init(PS, SL)
+    base = B.malloc(SL - (2 << 20))
+    B.fill_uniform(base, "float32", (16 << 20) // 4, 11, -1.0, 1.0)
+    B.fill_uniform(base + (16 << 20), "float64", (16 << 20) // 8, 12, -1.0, 1.0)
+    B.memset(base + (32 << 20), 0, 4096 * 8)
+    B.quiet()
+    for it in items:
+        it["dest"] += base
+        if "src" in it:
+            it["src"] += base
+    reqs = B.make_requests(items)
+    small = np.array([it["bytes"] <= 64 << 10 for it in items])
+
+    def pct(lat, mask=None):
+        x = lat if mask is None else lat[mask]
+        return {"p50_us": round(float(np.percentile(x, 50)) * 1e6, 2),
+                "p99_us": round(float(np.percentile(x, 99)) * 1e6, 2),
+                "p999_us": round(float(np.percentile(x, 99.9)) * 1e6, 2)}
+
+    srv = B.Server(queue_slots=SLOTS)
+    warm = min(2000, len(items))
+    srv.replay(B.make_requests(items[:warm]), arrival[:warm])  # warm-up stream
+    launches0 = B.launch_count()
+    t0 = time.perf_counter()
+    lat, fetched = srv.replay(reqs, arrival)
+    wall = time.perf_counter() - t0
+    launches = B.launch_count() - launches0
+    last = float(np.max(arrival + lat))
+    t0 = time.perf_counter()
+    lat_sat, _ = srv.replay(reqs, np.zeros(len(items)))
+    sat_s = float(np.max(lat_sat))
+    srv.stop()
+    npc = min(args.serve_percall, len(items))
+    pc_reqs = B.make_requests(items[:npc])
+    lat_pc, _ = B.replay(pc_reqs, arrival[:npc])
+    pc_last = float(np.max(arrival[:npc] + lat_pc))
+    lat_pc_sat, _ = B.replay(pc_reqs, np.zeros(npc))
+    pc_sat_s = float(np.max(lat_pc_sat))
+    total_bytes = int(sum(it["bytes"] for it in items))
+    line = {"metric": METRIC, "workload": "serve", "n_gpus": world,
+            "config": {"npes": PS, "arena_gib": PS * SL / 2 ** 30, "teams": "64 x 4 PEs",
+                       "requests": len(items), "arrival": "Poisson", "rate_per_s": args.serve_rate,
+                       "mix": "uniform over reduce/fcollect/alltoall/put/get/atomic",
+                       "payload": "log-uniform [8 B, 4 MiB] received per PE",
+                       "dtypes": "int32/int64/float32/float64", "queue_slots": SLOTS},
+            "served": {"latency_all": pct(lat), "latency_le_64KiB": pct(lat, small),
+                       "ops_per_s": round(len(items) / last, 1),
+                       "offered_per_s": round(len(items) / float(arrival[-1]), 1),
+                       "saturated_ops_per_s": round(len(items) / sat_s, 1),
+                       "saturated_gbs_received": round(total_bytes / sat_s / 1e9, 2),
+                       "kernel_launches": launches, "wall_s": round(wall, 3)},
+            "per_call": {"requests": npc, "latency_all": pct(lat_pc),
+                         "latency_le_64KiB": pct(lat_pc, small[:npc]),
+                         "ops_per_s": round(npc / pc_last, 1),
+                         "saturated_ops_per_s": round(npc / pc_sat_s, 1),
+                         "form": "one blocking b200shm_* call per request, in arrival order"},
+            "amo_fetch_adds": int(sum(1 for it in items if it["kind"] == "amo"))}
+    line["speedup_saturated_ops"] = round(line["served"]["saturated_ops_per_s"] /
+                                          line["per_call"]["saturated_ops_per_s"], 2)
     if rank == 0:
         print(json.dumps(line), flush=True)
 

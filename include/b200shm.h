@@ -262,6 +262,10 @@ int b200shm_serve_enqueue(b200shm_server *srv, const b200shm_request *req,
 /* 1 when the request completed (its AMO old value in *fetched, which may
  * be NULL), 0 while it is pending, < 0 on an error. */
 int b200shm_serve_poll(b200shm_server *srv, uint64_t ticket, uint64_t *fetched);
+/* Device clock stamps (globaltimer, ns) of a completed request still in
+ * its slot: copied from the ring into device memory, its last tiles
+ * claimed, complete.  1 when available, 0 otherwise. */
+int b200shm_serve_trace(b200shm_server *srv, uint64_t ticket, uint64_t stamps[3]);
 /* Block until the request completes or timeout_seconds pass
  * (B200SHM_ERR_TIMEOUT). */
 int b200shm_serve_wait(b200shm_server *srv, uint64_t ticket, double timeout_seconds,

@@ -79,6 +79,7 @@ def _load():
         "b200shm_serve_poll": (ci, [vp, u64, ctypes.POINTER(u64)]),
         "b200shm_serve_wait": (ci, [vp, u64, ctypes.c_double, ctypes.POINTER(u64)]),
         "b200shm_serve_stop": (ci, [vp]),
+        "b200shm_serve_trace": (ci, [vp, u64, vp]),
         "b200shm_serve_replay": (ci, [vp, vp, u64, vp, vp, vp]),
         "b200shm_amo": (ci, [ci, ci, ci, u64, vp, vp, vp]),
     }
@@ -337,6 +338,13 @@ class Server:
         f = ctypes.c_uint64()
         _check(lib.b200shm_serve_wait(self.h, ticket, timeout, ctypes.byref(f)))
         return f.value
+
+    def trace(self, ticket):
+        """Device times in ns (copied to the device, last claimed, done), or None."""
+        t = np.zeros(3, np.uint64)
+        if lib.b200shm_serve_trace(self.h, ticket, t.ctypes.data) != 1:
+            return None
+        return [int(v) for v in t]
 
     def replay(self, reqs, arrival_s):
         return replay(reqs, arrival_s, self)

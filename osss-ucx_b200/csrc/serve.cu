@@ -49,7 +49,7 @@ namespace {
 constexpr int kServeThreads = 256;
 constexpr int kTileBits = 24;
 constexpr unsigned long long kTileMask = (1ull << kTileBits) - 1;
-constexpr uint64_t kCopyChunk = 64u << 10;       /* bytes per copy tile            */
+constexpr uint64_t kCopyChunk = 32u << 10;       /* bytes per copy tile            */
 constexpr uint64_t kReduceTileRead = 256u << 10; /* source bytes per reduce tile   */
 
 /* A ring slot (mapped host memory, written by the host). */
@@ -65,13 +65,17 @@ struct alignas(16) SReq {
 };
 static_assert(sizeof(SReq) == 128, "ring slot of 128 bytes");
 
-/* A completion word (mapped host memory, written by the device). */
-struct alignas(32) SDone {
+/* A completion word (mapped host memory, written by the device), with the
+ * device clock (globaltimer, ns) when the request was copied from the
+ * ring, when its last tile was claimed and when it completed. */
+struct alignas(64) SDone {
   unsigned long long seq; /* ticket + 1 once complete */
   unsigned long long fetched;
+  unsigned long long t[3]; /* copied into device memory, last tiles claimed, complete */
   int status;
-  int pad[3];
+  int pad[5];
 };
+static_assert(sizeof(SDone) == 64, "completion record of 64 bytes");
 
 /* Host-written control words (mapped host memory). */
 struct SCtl {
@@ -82,10 +86,10 @@ struct SCtl {
 
 /* Device-side state. */
 struct SDev {
-  unsigned long long cursor;      /* next (request, tile) to hand out        */
+  unsigned long long cursor;      /* the request whose tiles are handed out  */
   unsigned long long tail_mirror; /* last tail a CTA read from host memory   */
-  unsigned int poll_lock;         /* one CTA at a time reads the host tail   */
-  unsigned int pad;
+  unsigned int poll_lock;         /* one CTA at a time reads host memory     */
+  int stop;                       /* the host's stop flag, as last read      */
 };
 
 struct SArgs {
@@ -94,8 +98,8 @@ struct SArgs {
   const SCtl *ctl;
   SDev *dev;
   unsigned int *tiles_done; /* per slot */
-  unsigned long long *mtag; /* per slot: ticket + 1 of the mirrored request, 0 while written */
-  SReq *mreq;               /* per slot: device copy of the request */
+  unsigned long long *tctr; /* per slot: (request << 24) | next tile, set when mirrored */
+  SReq *mreq;               /* per slot: device copy of the request (seq = ticket + 1) */
   unsigned int Q;
   char *base;
   uint64_t slice;
@@ -111,6 +115,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long
 __device__ __forceinline__ void st_release_sys(unsigned long long *p, unsigned long long v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+/* Release/acquire fences (lighter than the sequentially consistent
+ * __threadfence, which stalls behind the atomics of the waiting CTAs). */
+__device__ __forceinline__ void fence_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void fence_sys() { asm volatile("fence.acq_rel.sys;" ::: "memory"); }
 __device__ __forceinline__ unsigned long long vld(const unsigned long long *p) {
   return *(const volatile unsigned long long *)p;
 }
@@ -126,74 +134,85 @@ __device__ __forceinline__ void copy_words(SReq *dst, const SReq *src) {
   for (int i = 0; i < 16; i++) d[i] = s[i];
 }
 
-/* Read request r into *out (thread 0): 1 = consistent copy, 0 = the slot
- * was already recycled for a later request (so r is complete and all its
- * tiles were handed out), -1 = not visible yet.  The device mirror is a
- * seqlock: the tag is cleared, the copy written, the tag set. */
+/* The device mirror of the ring: the CTA that holds the poll lock copies
+ * newly published requests from host memory into it (sequence word last)
+ * before it advances tail_mirror, so the other CTAs read requests from L2
+ * only.  Read request r (< tail_mirror) into *out: 1 = a consistent copy,
+ * 0 = the slot already holds a later request (so r is complete and all its
+ * tiles were handed out). */
 __device__ int read_req(const SArgs &a, unsigned long long r, SReq *out) {
-  const unsigned slot = (unsigned)(r % a.Q);
-  if (vld(&a.mtag[slot]) == r + 1) {
-    __threadfence();
-    copy_words(out, &a.mreq[slot]);
-    __threadfence();
-    if (vld(&a.mtag[slot]) == r + 1) return 1;
-  }
-  const unsigned long long s1 = ld_acquire_sys(&a.ring[slot].seq);
-  if (s1 > r + 1) return 0;
-  if (s1 < r + 1) return -1;
-  copy_words(out, &a.ring[slot]);
-  __threadfence_system();
-  const unsigned long long s2 = ld_acquire_sys(&a.ring[slot].seq);
-  if (s2 != r + 1) return s2 > r + 1 ? 0 : -1;
-  *(volatile unsigned long long *)&a.mtag[slot] = 0;
-  __threadfence();
-  unsigned long long *d = (unsigned long long *)&a.mreq[slot];
-  const unsigned long long *w = (const unsigned long long *)out;
-  for (int i = 0; i < 16; i++) ((volatile unsigned long long *)d)[i] = w[i];
-  __threadfence();
-  *(volatile unsigned long long *)&a.mtag[slot] = r + 1;
-  return 1;
+  const SReq *m = &a.mreq[r % a.Q];
+  if (vld(&m->seq) != r + 1) return 0;
+  fence_gpu();
+  copy_words(out, m);
+  fence_gpu();
+  return vld(&m->seq) == r + 1 ? 1 : 0;
 }
 
-/* Claim the next tile (thread 0).  Returns 1 with *claimed = (r << 24 | t)
- * and the request in *req, or 0 when the CTA should exit (stop requested or
- * idle past the limit, in both cases with no published work unclaimed). */
-__device__ int claim(const SArgs &a, SReq *req, unsigned long long *claimed,
+constexpr unsigned long long kMirrorBatch = kServeThreads / 16; /* requests one poll copies */
+
+/* Claim the next tiles (thread 0).  Returns 1 with request *cr, tiles
+ * [*ct, *ct + *count) and the request in *req; 2 when this CTA took the poll
+ * lock and found requests [*mfrom, *mupto) published but not yet copied
+ * into device memory (the CTA copies them, then publishes and releases the
+ * lock); or 0 when the CTA should exit (stop requested or idle past the
+ * limit, in both cases holding no claim).
+ * Tiles come from a per-slot counter tagged with the request it serves, by
+ * fetch-and-add: every CTA gets a distinct share in one atomic.  An add that
+ * lands after the slot moved on to a later request x (only possible once
+ * the request it aimed at is complete) holds a share of x, which is served
+ * as such, so no tile is ever lost or handed out twice. */
+__device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned long long *ct,
+                     unsigned *count, unsigned long long *mfrom, unsigned long long *mupto,
                      unsigned long long idle_since) {
   unsigned backoff = 32;
   for (;;) {
-    const unsigned long long v = vld(&a.dev->cursor);
-    const unsigned long long r = v >> kTileBits, t = v & kTileMask;
+    const unsigned long long r = vld(&a.dev->cursor);
     unsigned long long tl = vld(&a.dev->tail_mirror);
     if (r >= tl) {
-      if (atomicCAS(&a.dev->poll_lock, 0u, 1u) == 0u) {
-        tl = ld_acquire_sys(&a.ctl->tail);
-        atomicMax(&a.dev->tail_mirror, tl);
+      /* test, then test-and-set: waiting CTAs only read the lock word */
+      if (*(const volatile unsigned *)&a.dev->poll_lock == 0u &&
+          atomicCAS(&a.dev->poll_lock, 0u, 1u) == 0u) {
+        const unsigned long long mt = vld(&a.dev->tail_mirror);
+        const unsigned long long ht = ld_acquire_sys(&a.ctl->tail);
+        if (*(const volatile int *)&a.ctl->stop) *(volatile int *)&a.dev->stop = 1;
+        if (ht > mt) { /* the whole CTA copies them, still holding the lock */
+          *mfrom = mt;
+          *mupto = ht < mt + kMirrorBatch ? ht : mt + kMirrorBatch;
+          return 2;
+        }
         atomicExch(&a.dev->poll_lock, 0u);
       }
       if (r >= tl) {
-        if (*(const volatile int *)&a.ctl->stop) return 0;
+        /* only the lock holder reads host memory: a read of host memory by
+         * every waiting CTA on every turn floods the path to the host and
+         * stalls every other memory access behind it */
+        if (*(const volatile int *)&a.dev->stop) return 0;
         if (now_ns() - idle_since > a.idle_ns) return 0;
         __nanosleep(backoff);
-        backoff = backoff < 1024 ? backoff * 2 : 1024;
+        backoff = backoff < 512 ? backoff * 2 : 512;
         continue;
       }
     }
-    const int rc = read_req(a, r, req);
-    if (rc < 0) {
-      if (now_ns() - idle_since > a.idle_ns) return 0;
-      __nanosleep(64);
+    fence_gpu();
+    if (req->seq != r + 1 && !read_req(a, r, req)) { /* recycled: r is complete */
+      atomicCAS(&a.dev->cursor, r, r + 1);
       continue;
     }
-    const unsigned long long nt = rc ? req->ntiles : 0;
-    if (t >= nt) {
-      atomicCAS(&a.dev->cursor, v, (r + 1) << kTileBits);
-      continue;
+    const unsigned long long k = (req->ntiles + gridDim.x - 1) / gridDim.x;
+    const unsigned long long old = atomicAdd(&a.tctr[r % a.Q], k);
+    const unsigned long long x = old >> kTileBits, c = old & kTileMask;
+    if (x != r) { /* the slot serves a later request x by now */
+      fence_gpu();
+      if (!read_req(a, x, req)) continue;
     }
-    if (atomicCAS(&a.dev->cursor, v, v + 1) == v) {
-      *claimed = v;
+    if (c < req->ntiles) {
+      *cr = x;
+      *ct = c;
+      *count = (unsigned)(req->ntiles - c < k ? req->ntiles - c : k);
       return 1;
     }
+    atomicCAS(&a.dev->cursor, r, r + 1); /* all of r's tiles are handed out */
   }
 }
 
@@ -209,80 +228,159 @@ __device__ __forceinline__ void stv(char *p, T v) {
   memcpy(p, &v, sizeof(T));
 }
 
-/* The tree the algorithm builds for float SUM/PROD (the value is the same
- * in every member, the ops being exactly commutative), leaves loaded four
- * at a time.  Binomial: op(upper block, lower block), then the set bits of
- * P from the lowest (reduce.c:137-154); butterfly: extra members folded as
- * op(extra, own), then log2(p2s) levels (reduce.c:206-272). */
+/* Where a float MIN/MAX result depends on operand order (a NaN, or both
+ * zeros, among the inputs): replay the algorithm's order for element e
+ * and write what each member receives (rec_dbl gives members different
+ * bits; the other algorithms give every member the block owner's). */
 template <class T, int OP>
-__device__ T tree_value(const char *s, uint64_t step, int P, int p2s, int logp2s, bool binomial) {
-  T stk[kMaxLevels + 1];
-  if (binomial) {
-    for (int j0 = 0; j0 < P; j0 += 4) {
-      T x[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (j0 + u < P) x[u] = ldv<T>(s + (uint64_t)(j0 + u) * step);
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (j0 + u < P) {
-          const int j = j0 + u;
-          T y = x[u];
-          for (int L = 0; L <= kMaxLevels; L++) {
-            if (j & (1 << L)) {
-              y = apply<OP>(y, stk[L]);
-            } else {
-              stk[L] = y;
-              break;
-            }
-          }
-        }
+__device__ void exact_element(int algo, const char *s, char *d, uint64_t step, int P, int p2s,
+                              int lg, uint64_t e, uint64_t N) {
+  auto get = [&](int j) { return ldv<T>(s + (uint64_t)j * step); };
+  const bool lower = e < N / 2;
+  if (algo == B200SHM_REC_DBL) {
+    for (int qq = 0; qq < p2s; qq++) {
+      const T x = exact_value<T, OP>(get, P, p2s, lg, algo, lower, qq);
+      const int as = p2s_member(qq, P, p2s);
+      stv<T>(d + (uint64_t)as * step, x);
+      if (p2s_extra(qq, P, p2s)) stv<T>(d + (uint64_t)(as + 1) * step, x);
     }
-    bool have = false;
-    T v = stk[0];
-    for (int L = 0; L <= kMaxLevels; L++)
-      if (P & (1 << L)) {
-        v = have ? apply<OP>(v, stk[L]) : stk[L];
-        have = true;
-      }
-    return v;
+    return;
   }
-  for (int q0 = 0; q0 < p2s; q0 += 4) {
-    T x[4], e[4];
+  int qq = 0;
+  if (algo == B200SHM_RABENSEIFNER || algo == B200SHM_RABENSEIFNER2)
+    qq = rev_bits(rab_block(e, N, p2s), lg);
+  const T x = exact_value<T, OP>(get, P, p2s, lg, algo, lower, qq);
+  for (int j = 0; j < P; j++) stv<T>(d + (uint64_t)j * step, x);
+}
+
+/* The tree the algorithm builds for float SUM/PROD, for one pack: the value
+ * is the same in every member, the ops being exactly commutative.  Leaves
+ * four at a time (own and extra members loaded together), a full batch
+ * pushed as a subtree of 4 into a binary counter whose levels combine
+ * earlier subtree first.  Binomial: op(upper block, lower block), then the
+ * set bits of P from the lowest (reduce.c:137-154); butterfly: extra
+ * members folded as op(extra, own), then log2(p2s) levels (reduce.c:
+ * 206-272). */
+template <class T, int V, int OP>
+__device__ Pack<T, V> tree_pack(const char *s, uint64_t step, int P, int p2s, int lg,
+                                bool binomial) {
+  typedef Pack<T, V> PK;
+  PK stk[kMaxLevels + 1];
+  int c = 0;
+  auto comb = [&](const PK &lo, const PK &hi) {
+    return binomial ? papply<OP>(hi, lo) : papply<OP>(lo, hi);
+  };
+  auto push = [&](PK v, int lv) {
+    const int t = __ffs(~(c >> lv)) - 1 + lv;
+    for (int L = lv; L < t; L++) v = comb(stk[L], v);
+    stk[t] = v;
+    c += 1 << lv;
+  };
+  const int nl = binomial ? P : p2s;
+  for (int qb = 0; qb < nl; qb += 4) {
+    const int k = nl - qb < 4 ? nl - qb : 4;
+    PK x[4], e[4];
     bool ex[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       ex[u] = false;
-      if (q0 + u < p2s) {
-        const int own = (int)(((long long)(q0 + u) * P + p2s - 1) >> logp2s);
-        const int nxt = (int)(((long long)(q0 + u + 1) * P + p2s - 1) >> logp2s);
-        x[u] = ldv<T>(s + (uint64_t)own * step);
-        ex[u] = nxt - own == 2;
-        if (ex[u]) e[u] = ldv<T>(s + (uint64_t)(own + 1) * step);
+      if (u < k) {
+        const int q = qb + u;
+        const int own = binomial ? q : (int)(((long long)q * P + p2s - 1) >> lg);
+        x[u] = ld_pack<T, V>(s + (uint64_t)own * step);
+        if (!binomial) {
+          ex[u] = (int)(((long long)(q + 1) * P + p2s - 1) >> lg) - own == 2;
+          if (ex[u]) e[u] = ld_pack<T, V>(s + (uint64_t)(own + 1) * step);
+        }
       }
     }
 #pragma unroll
     for (int u = 0; u < 4; u++)
-      if (q0 + u < p2s) {
-        const int leaf = q0 + u;
-        T y = ex[u] ? apply<OP>(e[u], x[u]) : x[u];
-        for (int L = 0; L <= kMaxLevels; L++) {
-          if (leaf & (1 << L)) {
-            y = apply<OP>(stk[L], y);
-          } else {
-            stk[L] = y;
-            break;
-          }
-        }
-      }
+      if (ex[u]) x[u] = papply<OP>(e[u], x[u]);
+    if (k == 4) {
+      push(comb(comb(x[0], x[1]), comb(x[2], x[3])), 2);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (u < k) push(x[u], 0);
+    }
   }
-  return stk[logp2s];
+  if (!binomial) return stk[lg];
+  bool have = false;
+  PK v = stk[0];
+  for (int L = 0; L <= kMaxLevels; L++)
+    if (P & (1 << L)) {
+      v = have ? comb(stk[L], v) : stk[L];
+      have = true;
+    }
+  return v;
 }
 
+/* Units [u0, u1) of V elements each, one per thread at a time, members
+ * loaded eight at a time. */
+template <class T, int V, int OP>
+__device__ void reduce_units(const b200shm_request &r, const char *src0, char *dst0,
+                             uint64_t step, uint64_t u0, uint64_t u1, int P, int p2s, int lg) {
+  typedef Pack<T, V> PK;
+  constexpr uint64_t UB = sizeof(T) * V;
+  constexpr bool FL = std::is_floating_point<T>::value;
+  constexpr bool MM = FL && (OP == B200SHM_MIN || OP == B200SHM_MAX);
+  const bool chain = !FL || MM || r.algo == B200SHM_LINEAR;
+  const bool bin = r.algo == B200SHM_BINOMIAL;
+  for (uint64_t k = u0 + threadIdx.x; k < u1; k += kServeThreads) {
+    const char *s = src0 + k * UB;
+    PK v;
+    unsigned cls[V];
+#pragma unroll
+    for (int i = 0; i < V; i++) cls[i] = 0;
+    if (chain) {
+      v = ld_pack<T, V>(s);
+      if constexpr (MM) {
+#pragma unroll
+        for (int i = 0; i < V; i++) cls[i] = fclass(v.x[i]);
+      }
+      for (int j = 1; j < P; j += 8) {
+        PK x[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++)
+          if (j + m < P) x[m] = ld_pack<T, V>(s + (uint64_t)(j + m) * step);
+#pragma unroll
+        for (int m = 0; m < 8; m++)
+          if (j + m < P) {
+            v = papply<OP>(v, x[m]);
+            if constexpr (MM) {
+#pragma unroll
+              for (int i = 0; i < V; i++) cls[i] |= fclass(x[m].x[i]);
+            }
+          }
+      }
+    } else {
+      v = tree_pack<T, V, OP>(s, step, P, p2s, lg, bin);
+    }
+    if constexpr (MM) {
+      bool amb = false;
+#pragma unroll
+      for (int i = 0; i < V; i++) amb |= ambiguous(cls[i]);
+      if (amb && r.algo != B200SHM_LINEAR) {
+        for (int i = 0; i < V; i++) {
+          const uint64_t e = k * V + i;
+          exact_element<T, OP>(r.algo, src0 + e * sizeof(T), dst0 + e * sizeof(T), step, P, p2s,
+                               lg, e, r.n);
+        }
+        continue;
+      }
+    }
+    char *d = dst0 + k * UB;
+    for (int j = 0; j < P; j++) st_pack<T, V>(d + (uint64_t)j * step, v);
+  }
+}
+
+/* Elements [e0, e1) of a reduction: 16-byte packs where the source and
+ * dest offsets allow (member strides are whole slices), then the rest. */
 template <class T, int OP>
-__device__ void serve_reduce(const SReq &q, uint64_t e0, uint64_t e1, char *base,
+__device__ void reduce_range(const b200shm_request &r, uint64_t e0, uint64_t e1, char *base,
                              uint64_t slice) {
-  const b200shm_request &r = q.r;
+  constexpr int V = (int)(16 / sizeof(T));
   const int P = r.pe_size;
   int p2s = 1, lg = 0;
   while (p2s * 2 <= P) {
@@ -292,96 +390,76 @@ __device__ void serve_reduce(const SReq &q, uint64_t e0, uint64_t e1, char *base
   const uint64_t step = (uint64_t)(P > 1 ? r.pe_stride : 1) * slice;
   const char *src0 = base + (uint64_t)r.pe_start * slice + r.src_off;
   char *dst0 = base + (uint64_t)r.pe_start * slice + r.dest_off;
-  constexpr bool FL = std::is_floating_point<T>::value;
-  constexpr bool MM = OP == B200SHM_MIN || OP == B200SHM_MAX;
-  const bool chain = !FL || MM || r.algo == B200SHM_LINEAR;
-  for (uint64_t e = e0 + threadIdx.x; e < e1; e += kServeThreads) {
-    const char *s = src0 + e * sizeof(T);
-    T v;
-    if (chain) {
-      v = ldv<T>(s);
-      unsigned cls = 0;
-      if constexpr (FL && MM) cls = fclass(v);
-      for (int j = 1; j < P; j += 8) {
-        T x[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-          if (j + u < P) x[u] = ldv<T>(s + (uint64_t)(j + u) * step);
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-          if (j + u < P) {
-            v = apply<OP>(v, x[u]);
-            if constexpr (FL && MM) cls |= fclass(x[u]);
-          }
-      }
-      if constexpr (FL && MM) {
-        /* order-dependent element: replay the algorithm's operand order
-         * (the left fold above already is the linear algorithm's) */
-        if (ambiguous(cls) && r.algo != B200SHM_LINEAR) {
-          auto get = [&](int j) { return ldv<T>(s + (uint64_t)j * step); };
-          const bool lower = e < r.n / 2;
-          if (r.algo == B200SHM_REC_DBL) {
-            for (int qq = 0; qq < p2s; qq++) {
-              const T x = exact_value<T, OP>(get, P, p2s, lg, r.algo, lower, qq);
-              const int as = p2s_member(qq, P, p2s);
-              stv<T>(dst0 + (uint64_t)as * step + e * sizeof(T), x);
-              if (p2s_extra(qq, P, p2s)) stv<T>(dst0 + (uint64_t)(as + 1) * step + e * sizeof(T), x);
-            }
-            continue;
-          }
-          int qq = 0;
-          if (r.algo == B200SHM_RABENSEIFNER || r.algo == B200SHM_RABENSEIFNER2)
-            qq = rev_bits(rab_block(e, r.n, p2s), lg);
-          v = exact_value<T, OP>(get, P, p2s, lg, r.algo, lower, qq);
-        }
-      }
-    } else {
-      v = tree_value<T, OP>(s, step, P, p2s, lg, r.algo == B200SHM_BINOMIAL);
-    }
-    char *d = dst0 + e * sizeof(T);
-    for (int j = 0; j < P; j++) stv<T>(d + (uint64_t)j * step, v);
+  uint64_t e = e0;
+  if (((r.src_off | r.dest_off) & 15) == 0 && e0 % V == 0) {
+    const uint64_t pend = e1 / V;
+    reduce_units<T, V, OP>(r, src0, dst0, step, e0 / V, pend, P, p2s, lg);
+    e = pend * V;
   }
+  if (e < e1) reduce_units<T, 1, OP>(r, src0, dst0, step, e, e1, P, p2s, lg);
 }
 
 template <class T>
-__device__ void serve_reduce_int(const SReq &q, uint64_t e0, uint64_t e1, char *base,
-                                 uint64_t slice) {
-  switch (q.r.op) {
-  case B200SHM_AND: serve_reduce<T, B200SHM_AND>(q, e0, e1, base, slice); break;
-  case B200SHM_OR: serve_reduce<T, B200SHM_OR>(q, e0, e1, base, slice); break;
-  case B200SHM_XOR: serve_reduce<T, B200SHM_XOR>(q, e0, e1, base, slice); break;
-  case B200SHM_MIN: serve_reduce<T, B200SHM_MIN>(q, e0, e1, base, slice); break;
-  case B200SHM_MAX: serve_reduce<T, B200SHM_MAX>(q, e0, e1, base, slice); break;
-  case B200SHM_SUM: serve_reduce<T, B200SHM_SUM>(q, e0, e1, base, slice); break;
-  default: serve_reduce<T, B200SHM_PROD>(q, e0, e1, base, slice); break;
-  }
-}
-template <class T>
-__device__ void serve_reduce_flt(const SReq &q, uint64_t e0, uint64_t e1, char *base,
-                                 uint64_t slice) {
-  switch (q.r.op) {
-  case B200SHM_MIN: serve_reduce<T, B200SHM_MIN>(q, e0, e1, base, slice); break;
-  case B200SHM_MAX: serve_reduce<T, B200SHM_MAX>(q, e0, e1, base, slice); break;
-  case B200SHM_SUM: serve_reduce<T, B200SHM_SUM>(q, e0, e1, base, slice); break;
-  default: serve_reduce<T, B200SHM_PROD>(q, e0, e1, base, slice); break;
+__device__ __noinline__ void serve_reduce(const SReq &q, uint64_t e0, uint64_t e1, char *base,
+                                          uint64_t slice) {
+  const b200shm_request &r = q.r;
+  if constexpr (std::is_floating_point<T>::value) {
+    switch (r.op) {
+    case B200SHM_MIN: reduce_range<T, B200SHM_MIN>(r, e0, e1, base, slice); break;
+    case B200SHM_MAX: reduce_range<T, B200SHM_MAX>(r, e0, e1, base, slice); break;
+    case B200SHM_SUM: reduce_range<T, B200SHM_SUM>(r, e0, e1, base, slice); break;
+    default: reduce_range<T, B200SHM_PROD>(r, e0, e1, base, slice); break;
+    }
+  } else {
+    switch (r.op) {
+    case B200SHM_AND: reduce_range<T, B200SHM_AND>(r, e0, e1, base, slice); break;
+    case B200SHM_OR: reduce_range<T, B200SHM_OR>(r, e0, e1, base, slice); break;
+    case B200SHM_XOR: reduce_range<T, B200SHM_XOR>(r, e0, e1, base, slice); break;
+    case B200SHM_MIN: reduce_range<T, B200SHM_MIN>(r, e0, e1, base, slice); break;
+    case B200SHM_MAX: reduce_range<T, B200SHM_MAX>(r, e0, e1, base, slice); break;
+    case B200SHM_SUM: reduce_range<T, B200SHM_SUM>(r, e0, e1, base, slice); break;
+    default: reduce_range<T, B200SHM_PROD>(r, e0, e1, base, slice); break;
+    }
   }
 }
 
 /* ---- copies ------------------------------------------------------------------ */
-/* Copy n bytes with threads [tid, tid + nthr) at the widest width that the
- * two addresses and the length allow. */
-__device__ void span_copy(char *dst, const char *src, uint64_t n, int tid, int nthr) {
-  const uint64_t al = (uint64_t)dst | (uint64_t)src | n;
-  if ((al & 15) == 0) {
-    for (uint64_t i = tid; i < n / 16; i += nthr) ((uint4 *)dst)[i] = ((const uint4 *)src)[i];
-  } else if ((al & 7) == 0) {
-    for (uint64_t i = tid; i < n / 8; i += nthr)
-      ((unsigned long long *)dst)[i] = ((const unsigned long long *)src)[i];
-  } else if ((al & 3) == 0) {
-    for (uint64_t i = tid; i < n / 4; i += nthr) ((unsigned *)dst)[i] = ((const unsigned *)src)[i];
-  } else {
-    for (uint64_t i = tid; i < n; i += nthr) dst[i] = src[i];
+template <class W>
+__device__ __forceinline__ void words_copy(W *d, const W *s, uint64_t n, int tid, int nthr) {
+  uint64_t i = tid;
+  const uint64_t st = (uint64_t)nthr;
+  for (; i + 7 * st < n; i += 8 * st) {
+    W x[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) x[u] = s[i + u * st];
+#pragma unroll
+    for (int u = 0; u < 8; u++) d[i + u * st] = x[u];
   }
+  for (; i < n; i += st) d[i] = s[i];
+}
+
+/* Copy n bytes with threads [tid, tid + nthr): bytes up to the dest's
+ * alignment, then the widest word the two addresses share an alignment
+ * for, four words in flight per thread, then the remaining bytes. */
+__device__ void span_copy(char *dst, const char *src, uint64_t n, int tid, int nthr) {
+  const uint64_t x = (uint64_t)dst ^ (uint64_t)src;
+  const uint64_t w = (x & 15) == 0 ? 16 : (x & 7) == 0 ? 8 : (x & 3) == 0 ? 4 : 1;
+  uint64_t head = (w - ((uint64_t)dst & (w - 1))) & (w - 1);
+  if (head > n) head = n;
+  for (uint64_t i = tid; i < head; i += nthr) dst[i] = src[i];
+  dst += head;
+  src += head;
+  n -= head;
+  const uint64_t nw = n / w;
+  switch (w) {
+  case 16: words_copy((uint4 *)dst, (const uint4 *)src, nw, tid, nthr); break;
+  case 8:
+    words_copy((unsigned long long *)dst, (const unsigned long long *)src, nw, tid, nthr);
+    break;
+  case 4: words_copy((unsigned *)dst, (const unsigned *)src, nw, tid, nthr); break;
+  default: words_copy((unsigned char *)dst, (const unsigned char *)src, nw, tid, nthr); break;
+  }
+  for (uint64_t i = nw * w + tid; i < n; i += nthr) dst[i] = src[i];
 }
 
 /* Segment s of a copy request: fcollect dest block k of member j <- member
@@ -407,7 +485,7 @@ __device__ void segment(const SReq &q, uint64_t s, char *base, uint64_t slice, c
   }
 }
 
-__device__ void serve_copy(const SReq &q, uint64_t t, char *base, uint64_t slice) {
+__device__ __noinline__ void serve_copy(const SReq &q, uint64_t t, char *base, uint64_t slice) {
   char *d;
   const char *s;
   if (q.spt == 0) { /* one chunk of one large segment: the whole CTA */
@@ -425,71 +503,121 @@ __device__ void serve_copy(const SReq &q, uint64_t t, char *base, uint64_t slice
   }
 }
 
+/* Copy ring slots [from, upto) from host memory into the device mirror,
+ * the whole CTA at once (one host word per thread, all reads in flight
+ * together), then publish them: sequence words, tile counters tagged with
+ * their request, tail_mirror; then release the poll lock (thread 0 holds
+ * it).  The sequence word is cleared before the copy is written, so a late
+ * reader of the slot's previous request sees the change. */
+__device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned long long upto) {
+  const unsigned n = (unsigned)(upto - from);
+  for (unsigned i = threadIdx.x; i < n; i += kServeThreads)
+    ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[14] = 0;
+  fence_gpu();
+  __syncthreads();
+  const unsigned long long now = now_ns();
+  for (unsigned w = threadIdx.x; w < n * 16; w += kServeThreads) {
+    const unsigned i = w >> 4, k = w & 15;
+    if (k == 14) continue;
+    const unsigned slot = (unsigned)((from + i) % a.Q);
+    const unsigned long long v =
+        k == 15 ? now : ((const volatile unsigned long long *)&a.ring[slot])[k];
+    ((volatile unsigned long long *)&a.mreq[slot])[k] = v;
+  }
+  fence_gpu();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (unsigned long long x = from; x < upto; x++)
+      ((volatile unsigned long long *)&a.mreq[x % a.Q])[14] = x + 1;
+    fence_gpu();
+    for (unsigned long long x = from; x < upto; x++) atomicExch(&a.tctr[x % a.Q], x << kTileBits);
+    fence_gpu();
+    *(volatile unsigned long long *)&a.dev->tail_mirror = upto;
+    fence_gpu();
+    atomicExch(&a.dev->poll_lock, 0u);
+  }
+  __syncthreads();
+}
+
 /* ---- the loop -------------------------------------------------------------------- */
 __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
   __shared__ SReq s_req;
-  __shared__ unsigned long long s_claim;
+  __shared__ unsigned long long s_cr, s_ct, s_mfrom, s_mupto;
+  __shared__ unsigned s_count;
   __shared__ int s_go;
   __shared__ unsigned long long s_fetched;
   __shared__ int s_status;
+  __shared__ unsigned long long s_tclaim;
   unsigned long long idle_since = now_ns();
+  if (threadIdx.x == 0) s_req.seq = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      s_go = claim(a, &s_req, &s_claim, idle_since);
+      s_go = claim(a, &s_req, &s_cr, &s_ct, &s_count, &s_mfrom, &s_mupto, idle_since);
+      s_tclaim = now_ns();
       s_fetched = 0;
       s_status = 0;
     }
     __syncthreads();
     if (!s_go) return;
-    const unsigned long long r = s_claim >> kTileBits, t = s_claim & kTileMask;
+    if (s_go == 2) {
+      mirror_ring(a, s_mfrom, s_mupto);
+      idle_since = now_ns();
+      continue;
+    }
+    const unsigned long long r = s_cr, t0 = s_ct;
     const SReq &q = s_req;
-    switch (q.r.kind) {
-    case B200SHM_REQ_REDUCE: {
-      const uint64_t e0 = t * q.unit;
-      const uint64_t e1 = e0 + q.unit < q.r.n ? e0 + q.unit : q.r.n;
-      switch (q.r.dtype) {
-      case B200SHM_I32: serve_reduce_int<int32_t>(q, e0, e1, a.base, a.slice); break;
-      case B200SHM_U32: serve_reduce_int<uint32_t>(q, e0, e1, a.base, a.slice); break;
-      case B200SHM_I64: serve_reduce_int<int64_t>(q, e0, e1, a.base, a.slice); break;
-      case B200SHM_U64: serve_reduce_int<uint64_t>(q, e0, e1, a.base, a.slice); break;
-      case B200SHM_F32: serve_reduce_flt<float>(q, e0, e1, a.base, a.slice); break;
-      case B200SHM_F64: serve_reduce_flt<double>(q, e0, e1, a.base, a.slice); break;
+    for (unsigned long long t = t0; t < t0 + s_count; t++) {
+      switch (q.r.kind) {
+      case B200SHM_REQ_REDUCE: {
+        const uint64_t e0 = t * q.unit;
+        const uint64_t e1 = e0 + q.unit < q.r.n ? e0 + q.unit : q.r.n;
+        switch (q.r.dtype) {
+        case B200SHM_I32: serve_reduce<int32_t>(q, e0, e1, a.base, a.slice); break;
+        case B200SHM_U32: serve_reduce<uint32_t>(q, e0, e1, a.base, a.slice); break;
+        case B200SHM_I64: serve_reduce<int64_t>(q, e0, e1, a.base, a.slice); break;
+        case B200SHM_U64: serve_reduce<uint64_t>(q, e0, e1, a.base, a.slice); break;
+        case B200SHM_F32: serve_reduce<float>(q, e0, e1, a.base, a.slice); break;
+        case B200SHM_F64: serve_reduce<double>(q, e0, e1, a.base, a.slice); break;
+        default:
+          if (threadIdx.x == 0) s_status = B200SHM_STATUS_BADREQ;
+        }
+        break;
+      }
+      case B200SHM_REQ_FCOLLECT:
+      case B200SHM_REQ_ALLTOALL:
+      case B200SHM_REQ_PUT:
+      case B200SHM_REQ_GET: serve_copy(q, t, a.base, a.slice); break;
+      case B200SHM_REQ_AMO:
+        if (threadIdx.x == 0) {
+          char *p = a.base + (uint64_t)q.r.pe * a.slice + q.r.dest_off;
+          const bool w8 = q.r.dtype == B200SHM_I64 || q.r.dtype == B200SHM_U64 ||
+                          q.r.dtype == B200SHM_F64;
+          if (w8)
+            s_fetched = amo_one<unsigned long long>(q.r.op, (unsigned long long *)p, q.r.value,
+                                                    q.r.cond);
+          else
+            s_fetched = amo_one<unsigned int>(q.r.op, (unsigned int *)p,
+                                              (unsigned int)q.r.value, (unsigned int)q.r.cond);
+        }
+        break;
       default:
         if (threadIdx.x == 0) s_status = B200SHM_STATUS_BADREQ;
       }
-      break;
     }
-    case B200SHM_REQ_FCOLLECT:
-    case B200SHM_REQ_ALLTOALL:
-    case B200SHM_REQ_PUT:
-    case B200SHM_REQ_GET: serve_copy(q, t, a.base, a.slice); break;
-    case B200SHM_REQ_AMO:
-      if (threadIdx.x == 0) {
-        char *p = a.base + (uint64_t)q.r.pe * a.slice + q.r.dest_off;
-        const bool w8 = q.r.dtype == B200SHM_I64 || q.r.dtype == B200SHM_U64 ||
-                        q.r.dtype == B200SHM_F64;
-        if (w8)
-          s_fetched = amo_one<unsigned long long>(q.r.op, (unsigned long long *)p, q.r.value,
-                                                  q.r.cond);
-        else
-          s_fetched = amo_one<unsigned int>(q.r.op, (unsigned int *)p, (unsigned int)q.r.value,
-                                            (unsigned int)q.r.cond);
-      }
-      break;
-    default:
-      if (threadIdx.x == 0) s_status = B200SHM_STATUS_BADREQ;
-    }
-    __threadfence();
+    fence_gpu();
     __syncthreads();
     if (threadIdx.x == 0) {
       const unsigned slot = (unsigned)(r % a.Q);
-      __threadfence_system();
-      if (atomicAdd(&a.tiles_done[slot], 1u) + 1ull == q.ntiles) {
+      fence_gpu();
+      if (atomicAdd(&a.tiles_done[slot], s_count) + (unsigned long long)s_count == q.ntiles) {
+        fence_sys();
         a.tiles_done[slot] = 0;
         SDone *dn = &a.done[slot];
         *(volatile unsigned long long *)&dn->fetched = s_fetched;
+        *(volatile unsigned long long *)&dn->t[0] = q.pad;
+        *(volatile unsigned long long *)&dn->t[1] = s_tclaim;
+        *(volatile unsigned long long *)&dn->t[2] = now_ns();
         *(volatile int *)&dn->status = s_status;
-        __threadfence_system();
         st_release_sys(&dn->seq, r + 1);
       }
     }
@@ -638,7 +766,10 @@ int plan_request(const b200shm_request &r0, SReq *q) {
     }
     if (q->ntiles == 0) q->ntiles = 1;
   }
-  if (q->ntiles > kTileMask) return fail(B200SHM_ERR_ARG, "serve: request of more than 2^24 tiles");
+  /* shares handed out past the last tile stay below twice the tiles plus
+   * one share per CTA, inside the counter's 24 bits */
+  if (q->ntiles > (kTileMask >> 2))
+    return fail(B200SHM_ERR_ARG, "serve: request of more than 2^22 tiles");
   return B200SHM_OK;
 }
 
@@ -699,8 +830,8 @@ int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
   a.ctl = s->d_ctl;
   a.dev = (SDev *)s->d_mem;
   a.mreq = (SReq *)(s->d_mem + 256);
-  a.mtag = (unsigned long long *)(s->d_mem + 256 + (size_t)s->Q * sizeof(SReq));
-  a.tiles_done = (unsigned *)(a.mtag + s->Q);
+  a.tctr = (unsigned long long *)(s->d_mem + 256 + (size_t)s->Q * sizeof(SReq));
+  a.tiles_done = (unsigned *)(a.tctr + s->Q);
   a.Q = s->Q;
   a.base = st().base;
   a.slice = st().slice;
@@ -750,6 +881,15 @@ int b200shm_serve_poll(b200shm_server *s, uint64_t ticket, uint64_t *fetched) {
   const int status = *(const volatile int *)&d->status;
   if (status) return fail(B200SHM_ERR_ARG, "serve: request %llu was refused on the device",
                           (unsigned long long)ticket);
+  return 1;
+}
+
+int b200shm_serve_trace(b200shm_server *s, uint64_t ticket, uint64_t stamps[3]) {
+  if (!s || !stamps) return fail(B200SHM_ERR_ARG, "serve_trace: null argument");
+  const SDone *d = &s->h_done[ticket % s->Q];
+  if (*(const volatile unsigned long long *)&d->seq != ticket + 1) return 0;
+  std::atomic_thread_fence(std::memory_order_acquire);
+  for (int i = 0; i < 3; i++) stamps[i] = ((const volatile unsigned long long *)d->t)[i];
   return 1;
 }
 
