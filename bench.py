@@ -217,6 +217,9 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200000.0, help="arrivals per second")
     ap.add_argument("--serve-percall", type=int, default=20000,
                     help="requests replayed through the per-call entry points")
+    ap.add_argument("--batch-npes", type=int, default=2048)
+    ap.add_argument("--batch-teams", type=int, default=512)
+    ap.add_argument("--batch-reductions", type=int, default=4096)
     ap.add_argument("--batch-tune", default="auto", choices=["auto", "off"],
                     help="batch workload: autotune lanes/tile per shape class, or heuristic plan")
     args = ap.parse_args()
@@ -477,10 +480,12 @@ def batch_workload(seed=4, PB=2048, NT=512, NR=4096):
     keeps the busiest PE's share of the heap smallest."""
     rng = np.random.default_rng(seed)
     u = rng.random(NT)
-    sizes = np.clip((1.0 / (0.5 - u * (0.5 - 1 / 256))).astype(int), 2, 256)
+    sizes = np.clip((1.0 / (0.5 - u * (0.5 - 1 / 256))).astype(int), 2, min(256, PB))
     teams, pos = [], 0
     for k, sz in enumerate(sizes):
         stride = [1, 2, 4][k % 3]
+        while stride > 1 and (int(sz) - 1) * stride + 1 > PB:
+            stride //= 2  # only for arenas smaller than the configuration's 2048 PEs
         span = (int(sz) - 1) * stride + 1
         teams.append((pos % (PB - span + 1), stride, int(sz)))
         pos += span
@@ -521,8 +526,8 @@ def run_batch(args, world, rank, local):
     import __graft_entry__
     __graft_entry__.build_library()
     import b200shm as B
-    PB = 2048
-    items, heap_need, sizes = batch_workload()
+    PB = args.batch_npes
+    items, heap_need, sizes = batch_workload(PB=PB, NT=args.batch_teams, NR=args.batch_reductions)
     B.init(PB, heap_need + (2 << 20))
     region = B.malloc(heap_need)
     for k, it in enumerate(items):
@@ -574,7 +579,7 @@ def run_batch(args, world, rank, local):
     peak, peak_kind = peaks()
     line = {"metric": METRIC, "workload": "batch", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup,
-            "config": {"npes": PB, "teams": 512, "team_size_alpha": 2,
+            "config": {"npes": PB, "teams": args.batch_teams, "team_size_alpha": 2,
                        "team_size_mean": round(float(sizes.mean()), 2),
                        "team_size_max": int(sizes.max()), "reductions": len(items),
                        "nelems": "log-uniform [16, 2^18]", "dtypes": "int32/int64/float32/float64",
@@ -590,7 +595,7 @@ def run_batch(args, world, rank, local):
                                                        minlength=9).tolist()},
             "per_call": {"ms": round(pc_ms, 4), "ops_per_s": round(len(items) / (pc_ms / 1e3), 1),
                          "gbs": round(total_bytes / (pc_ms / 1e3) / 1e9, 1),
-                         "form": "4096 b200shm_reduce calls, stream-ordered"},
+                         "form": "%d b200shm_reduce calls, stream-ordered" % len(items)},
             "speedup": round(pc_ms / b_ms, 2), "alg_bytes": total_bytes,
             "hbm_floor_ms": round(total_bytes / (peak * 1e9) * 1e3, 4), "peak_kind": peak_kind,
             "batch_matches_per_call": bool(match), "gpu_launches_per_batch": launches}
@@ -708,6 +713,12 @@ def run_serve(args, world, rank, local):
     lat, fetched = srv.replay(reqs, arrival)
     wall = time.perf_counter() - t0
     launches = B.launch_count() - launches0
+    # device clock stamps of the last queue-full of requests (still in their slots)
+    first = warm + len(items) - SLOTS
+    tr = np.array([srv.trace(t) for t in range(first, warm + len(items))], dtype=np.float64)
+    stages = {"mirrored_to_claimed_us_p50": round(float(np.median(tr[:, 1] - tr[:, 0])) / 1e3, 2),
+              "claimed_to_done_us_p50": round(float(np.median(tr[:, 2] - tr[:, 1])) / 1e3, 2),
+              "requests": SLOTS}
     last = float(np.max(arrival + lat))
     t0 = time.perf_counter()
     lat_sat, _ = srv.replay(reqs, np.zeros(len(items)))
@@ -731,7 +742,8 @@ def run_serve(args, world, rank, local):
                        "offered_per_s": round(len(items) / float(arrival[-1]), 1),
                        "saturated_ops_per_s": round(len(items) / sat_s, 1),
                        "saturated_gbs_received": round(total_bytes / sat_s / 1e9, 2),
-                       "kernel_launches": launches, "wall_s": round(wall, 3)},
+                       "kernel_launches": launches, "wall_s": round(wall, 3),
+                       "device_stages": stages},
             "per_call": {"requests": npc, "latency_all": pct(lat_pc),
                          "latency_le_64KiB": pct(lat_pc, small[:npc]),
                          "ops_per_s": round(npc / pc_last, 1),
