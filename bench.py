@@ -339,9 +339,13 @@ def main():
             h2d = d2h = 0
             for op, dt, algo, so, npdt, i in calls:
                 nb = xs[i][0].nbytes
-                B.lib.b200shm_put_host(0, 1, P, so, pinned_in[i].data_ptr(), nb, stream_ptr)
-                B.reduce(op, dt, algo, dst, so, N, team=team, stream=stream_ptr)
-                B.lib.b200shm_get_host(pinned_out[i].data_ptr(), 0, 1, P, dst, nb, stream_ptr)
+                rc = B.lib.b200shm_reduce_host(B.OPS.index(op), B.DTYPES.index(dt),
+                                               B.ALGOS.index(algo), 0, 1, P,
+                                               pinned_out[i].data_ptr(), nb,
+                                               pinned_in[i].data_ptr(), nb, dst, so, N,
+                                               stream_ptr)
+                if rc:
+                    raise B.B200Error(rc, B.lib.b200shm_last_error().decode())
                 h2d += P * nb
                 d2h += P * nb
         e2e_step()
@@ -362,7 +366,8 @@ def main():
         e2e = {"value": round(step_bytes * args.e2e_steps * world / (ems / 1e3) / 1e9, 3),
                "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "steps": args.e2e_steps, "ms_per_step": round(ems / args.e2e_steps, 3),
-               "path": "b200shm_put_host -> b200shm_reduce -> b200shm_get_host, pinned host rows"}
+               "path": "b200shm_reduce_host (pinned host rows in and out; copy in, reduce and "
+                       "copy out pipelined in chunks on three streams)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -102,6 +102,21 @@ int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_stride,
                    int pe_size, uint64_t dest_off, uint64_t src_off,
                    uint64_t nelems, void *stream);
 
+/* The all-reduce of host rows: member i's source row is host_src +
+ * i*src_pitch and its result row host_dest + i*dest_pitch (bytes); the rows
+ * pass through the symmetric objects at src_off / dest_off.  The same as
+ * b200shm_put_host(src rows) + b200shm_reduce + b200shm_get_host(dest rows),
+ * and bit-identical to it, but pipelined: the elements go in chunks whose
+ * copy in, reduction and copy out overlap on three streams, so both PCIe
+ * directions and the GPU work at once (pinned host rows are needed for the
+ * copies to overlap).  Replaces the reference's put + shcoll reduce + get
+ * sequence of a host-resident caller (src/shmemc/ucx/comms.c:677-737,
+ * src/shcoll/src/reduce.c:1078-1102). */
+int b200shm_reduce_host(int op, int dtype, int algo, int pe_start, int pe_stride,
+                        int pe_size, void *host_dest, uint64_t dest_pitch,
+                        const void *host_src, uint64_t src_pitch, uint64_t dest_off,
+                        uint64_t src_off, uint64_t nelems, void *stream);
+
 /* The same all-reduce for callers that cannot allocate device memory (a
  * runtime that owns every device allocation through its own pool, or code
  * that may not call cudaMalloc at all).  No counterpart in the reference.

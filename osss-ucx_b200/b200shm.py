@@ -62,6 +62,7 @@ def _load():
         "b200shm_memset": (ci, [ci, ci, ci, u64, ci, u64, vp]),
         "b200shm_reduce": (ci, [ci, ci, ci, ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_reduce_noalloc": (ci, [ci, ci, ci, ci, vp, u64, vp, u64, u64, vp]),
+        "b200shm_reduce_host": (ci, [ci, ci, ci, ci, ci, ci, vp, u64, vp, u64, u64, u64, u64, vp]),
         "b200shm_fcollect": (ci, [ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_alltoall": (ci, [ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_alltoalls": (ci, [ci, ci, ci, u64, u64, i64, i64, u64, u64, vp]),
@@ -177,6 +178,19 @@ def reduce(op, dtype, algo, dest, src, nelems, team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_reduce(OPS.index(op), DTYPES.index(dtype), ALGOS.index(algo),
                                      start, stride, size, dest, src, nelems, stream))
+
+
+def reduce_host(op, dtype, algo, dest, src, x, out=None, team=None, stream=None):
+    """All-reduce of host rows x[i] (member i) through the objects at src/dest;
+    returns (or fills) the host result rows.  Pinned arrays let the copies overlap."""
+    start, stride, size = _team(team)
+    x = np.ascontiguousarray(x)
+    if out is None:
+        out = np.empty_like(x)
+    _check(lib.b200shm_reduce_host(OPS.index(op), DTYPES.index(dtype), ALGOS.index(algo), start,
+                                   stride, size, out.ctypes.data, out[0].nbytes, x.ctypes.data,
+                                   x[0].nbytes, dest, src, x.shape[1], stream))
+    return out
 
 
 def reduce_noalloc(op, dtype, algo, npes, dest_ptr, dest_stride, src_ptr, src_stride, nelems,

@@ -35,6 +35,7 @@
 #include <string.h>
 
 #include <mutex>
+#include <vector>
 #include <type_traits>
 
 #include "internal.cuh"
@@ -60,7 +61,8 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
     for (int j = threadIdx.x; j < a.P; j += blockDim.x)
       memcpy(&vals[j], a.src + (uint64_t)j * a.sstep + e * sizeof(T), sizeof(T));
     __syncthreads();
-    const bool lower = e < a.N / 2;
+    const uint64_t eg = a.g_off + e; /* the order depends on the position in the whole */
+    const bool lower = eg < a.g_n / 2;
     if (a.algo == B200SHM_REC_DBL) {
       /* every p2s member (and the extra folded into it) keeps its own value */
       for (int q = threadIdx.x; q < a.p2s; q += blockDim.x) {
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
       if (threadIdx.x == 0) {
         int q = 0;
         if (a.algo != B200SHM_LINEAR && a.algo != B200SHM_BINOMIAL)
-          q = rev_bits(rab_block(e, a.N, a.p2s), a.logp2s); /* owner of e's block */
+          q = rev_bits(rab_block(eg, a.g_n, a.p2s), a.logp2s); /* owner of e's block */
         common = exact_value<T, OP>([&](int j) { return vals[j]; }, a.P, a.p2s, a.logp2s, a.algo,
                                     lower, q);
       }
@@ -568,6 +570,8 @@ static RArgs reduce_args(const char *src, char *dst, uint64_t sstep, uint64_t ds
   a.e_begin = 0;
   a.nvec = 0;
   a.N = nelems;
+  a.g_off = 0;
+  a.g_n = nelems;
   a.P = P;
   a.p2s = p2s;
   a.logp2s = logp;
@@ -598,6 +602,27 @@ int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int 
   a.fix_cap = st().fix_cap;
   a.status = st().d_status;
   const bool aligned = ((src_off | dest_off | m.step) & 15u) == 0;
+  return reduce_dispatch(op, dtype, a, aligned, s);
+}
+
+/* Elements [e0, e0 + count) of a reduction of nelems elements (validated by
+ * the caller), as one more launch sequence on stream s: the per-element
+ * result is that of the whole reduction. */
+int reduce_range_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
+                        uint64_t dest_off, uint64_t src_off, uint64_t nelems, uint64_t e0,
+                        uint64_t count, cudaStream_t s) {
+  if (count == 0) return B200SHM_OK;
+  const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  Members m = members(pe_start, pe_stride, pe_size);
+  RArgs a = reduce_args(m.first + src_off + e0 * es, m.first + dest_off + e0 * es, m.step, m.step,
+                        pe_size, count, algo);
+  a.g_off = e0;
+  a.g_n = nelems;
+  a.fix_list = st().fix_list;
+  a.fix_count = st().fix_count;
+  a.fix_cap = st().fix_cap;
+  a.status = st().d_status;
+  const bool aligned = (((src_off + e0 * es) | (dest_off + e0 * es) | m.step) & 15u) == 0;
   return reduce_dispatch(op, dtype, a, aligned, s);
 }
 
@@ -643,6 +668,100 @@ extern "C" int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_
                                nelems, b200::pick_stream(stream));
   if (rc) return rc;
   return b200::finish(stream, "b200shm_reduce");
+}
+
+/* ---------------------------------------------------------------------------
+ * b200shm_reduce_host: put_host + reduce + get_host of host rows, pipelined.
+ * The elements are cut into chunks; chunk c's copy in (one 2-D copy for all
+ * members), its reduction and its copy out run on three streams joined by
+ * events, so the copy engines move chunk c+1 in and chunk c-1 out while
+ * chunk c is reduced.  A chunk's results are those of the whole reduction
+ * (the global element index is kept for the order-dependent elements).
+ * ------------------------------------------------------------------------- */
+namespace b200 {
+namespace {
+struct HostPipe {
+  cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+  std::vector<cudaEvent_t> ev;
+  std::mutex mu;
+};
+HostPipe &host_pipe() {
+  static HostPipe p;
+  return p;
+}
+int pipe_events(HostPipe &p, size_t n) {
+  while (p.ev.size() < n) {
+    cudaEvent_t e;
+    B200_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p.ev.push_back(e);
+  }
+  return B200SHM_OK;
+}
+}  // namespace
+}  // namespace b200
+
+extern "C" int b200shm_reduce_host(int op, int dtype, int algo, int pe_start, int pe_stride,
+                                   int pe_size, void *host_dest, uint64_t dest_pitch,
+                                   const void *host_src, uint64_t src_pitch, uint64_t dest_off,
+                                   uint64_t src_off, uint64_t nelems, void *stream) {
+  using namespace b200;
+  int rc = check_team(pe_start, pe_stride, pe_size);
+  if (rc) return rc;
+  if ((rc = reduce_check(op, dtype, algo, pe_size))) return rc;
+  const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  if (nelems > st().slice / es) return fail(B200SHM_ERR_ARG, "reduce_host: nelems too large");
+  const uint64_t bytes = nelems * es;
+  if ((rc = check_extent(src_off, bytes, "reduce_host source")) ||
+      (rc = check_extent(dest_off, bytes, "reduce_host dest")))
+    return rc;
+  if (dest_off != src_off && overlaps(dest_off, bytes, src_off, bytes))
+    return fail(B200SHM_ERR_ARG, "reduce_host: dest and source overlap without being identical");
+  if (nelems == 0) return B200SHM_OK;
+  if (!host_dest || !host_src || dest_pitch < bytes || src_pitch < bytes)
+    return fail(B200SHM_ERR_ARG, "reduce_host: null host row or pitch below the row size");
+  /* chunks of about 32 MiB over all members (B200SHM_HOST_CHUNK_BYTES overrides),
+   * a whole number of 4 KiB per member */
+  uint64_t target = 32ull << 20;
+  if (const char *e = getenv("B200SHM_HOST_CHUNK_BYTES")) target = strtoull(e, nullptr, 0);
+  uint64_t chunk = target / ((uint64_t)pe_size * es);
+  chunk = chunk / (4096 / es) * (4096 / es);
+  if (chunk < 4096 / es) chunk = 4096 / es;
+  const uint64_t nch = (nelems + chunk - 1) / chunk;
+  HostPipe &p = host_pipe();
+  std::lock_guard<std::mutex> lk(p.mu);
+  if (!p.in) {
+    B200_CK(cudaStreamCreateWithFlags(&p.in, cudaStreamNonBlocking));
+    B200_CK(cudaStreamCreateWithFlags(&p.comp, cudaStreamNonBlocking));
+    B200_CK(cudaStreamCreateWithFlags(&p.out, cudaStreamNonBlocking));
+  }
+  if ((rc = pipe_events(p, 2 * nch + 2))) return rc;
+  cudaStream_t caller = pick_stream(stream);
+  /* start after the caller's earlier work */
+  B200_CK(cudaEventRecord(p.ev[2 * nch], caller));
+  B200_CK(cudaStreamWaitEvent(p.in, p.ev[2 * nch], 0));
+  B200_CK(cudaStreamWaitEvent(p.comp, p.ev[2 * nch], 0));
+  const Members m = members(pe_start, pe_stride, pe_size);
+  const uint64_t pitch = m.step ? m.step : st().slice;
+  for (uint64_t c = 0; c < nch; c++) {
+    const uint64_t e0 = c * chunk, cnt = nelems - e0 < chunk ? nelems - e0 : chunk;
+    B200_CK(cudaMemcpy2DAsync(m.first + src_off + e0 * es, pitch,
+                              (const char *)host_src + e0 * es, src_pitch, cnt * es, pe_size,
+                              cudaMemcpyHostToDevice, p.in));
+    B200_CK(cudaEventRecord(p.ev[2 * c], p.in));
+    B200_CK(cudaStreamWaitEvent(p.comp, p.ev[2 * c], 0));
+    if ((rc = reduce_range_launch(op, dtype, algo, pe_start, pe_stride, pe_size, dest_off,
+                                  src_off, nelems, e0, cnt, p.comp)))
+      return rc;
+    B200_CK(cudaEventRecord(p.ev[2 * c + 1], p.comp));
+    B200_CK(cudaStreamWaitEvent(p.out, p.ev[2 * c + 1], 0));
+    B200_CK(cudaMemcpy2DAsync((char *)host_dest + e0 * es, dest_pitch,
+                              m.first + dest_off + e0 * es, pitch, cnt * es, pe_size,
+                              cudaMemcpyDeviceToHost, p.out));
+  }
+  /* the caller's stream continues after the last copy out */
+  B200_CK(cudaEventRecord(p.ev[2 * nch + 1], p.out));
+  B200_CK(cudaStreamWaitEvent(caller, p.ev[2 * nch + 1], 0));
+  return finish(stream, "b200shm_reduce_host");
 }
 
 /* ---------------------------------------------------------------------------

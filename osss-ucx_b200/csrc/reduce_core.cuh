@@ -200,7 +200,9 @@ struct RArgs {
   uint64_t dstep;   /* same for dest (equal; kept separate)    */
   uint64_t e_begin; /* first element of this launch            */
   uint64_t nvec;    /* packs in this launch                    */
-  uint64_t N;       /* elements of the whole reduction         */
+  uint64_t N;       /* elements of this view                   */
+  uint64_t g_off;   /* the view's element 0 in the whole reduction */
+  uint64_t g_n;     /* elements of the whole reduction         */
   int P, p2s, logp2s, algo;
   unsigned long long *fix_list, *fix_count; /* deferred elements */
   unsigned long long fix_cap;
