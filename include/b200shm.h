@@ -142,6 +142,16 @@ int b200shm_fcollect(int pe_start, int pe_stride, int pe_size,
                      uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
                      void *stream);
 
+/* Variable-size allgather: member k contributes nbytes[k] bytes (host
+ * array of pe_size sizes) from src_off; every member's dest holds the
+ * contributions concatenated in member order (member k's block at the sum
+ * of nbytes[0..k)).  Replaces collect_helper_* (src/shcoll/src/collect.c:
+ * 35-591) behind shcoll_collect{32,64}_<algo>, shcoll_<T>_collect_<algo> and
+ * shcoll_collectmem_<algo> (collect.c:593-738), where each PE passes its own
+ * count. */
+int b200shm_collect(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                    uint64_t src_off, const uint64_t *nbytes, void *stream);
+
 /* All-to-all of nbytes blocks: member j's dest block k = member k's source
  * block j.  Replaces alltoall_helper_* (src/shcoll/src/alltoall.c:75-201)
  * behind shcoll_alltoall{32,64}_<algo>, shcoll_<T>_alltoall_<algo> and

@@ -8,7 +8,7 @@
  * (shmem_malloc/free/calloc/align, shmem_ptr), put/get/p/g, fence/quiet,
  * barrier_all/sync_all/barrier/sync/team_sync, the reductions
  * (shmem_<T>_<op>_reduce and shmem_<T>_<op>_to_all over the reference's type
- * tables), fcollect / broadcast / alltoall / alltoalls in their typed, mem
+ * tables), fcollect / collect / broadcast / alltoall / alltoalls in their typed, mem
  * and 32/64 forms, the atomics (shmem_[ctx_]<T>_atomic_*), and teams
  * (world, split_strided, split_2d, my_pe, n_pes, translate, destroy).
  *
@@ -189,6 +189,8 @@ SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_PROD)
 #define SHMEM_B200_DECL_COPY(_type, _tn)                                        \
   int shmem_##_tn##_fcollect(shmem_team_t team, _type *dest,                   \
                              const _type *source, size_t nelems);               \
+  int shmem_##_tn##_collect(shmem_team_t team, _type *dest,                    \
+                            const _type *source, size_t nelems);                \
   int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                   \
                              const _type *source, size_t nelems);               \
   int shmem_##_tn##_alltoalls(shmem_team_t team, _type *dest,                  \
@@ -204,6 +206,9 @@ SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_PROD)
   _type shmem_##_tn##_g(const _type *source, int pe);
 SHMEM_B200_RMA_TYPES(SHMEM_B200_DECL_COPY)
 int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
+/* collect: each PE passes its own nelems; dest gets the contributions
+ * concatenated in member order (shcoll-shim.c:471-560) */
+int shmem_collectmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
 int shmem_alltoallmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
 int shmem_alltoallsmem(shmem_team_t team, void *dest, const void *source, ptrdiff_t dst,
                        ptrdiff_t sst, size_t nelems);
@@ -213,6 +218,10 @@ void shmem_fcollect32(void *target, const void *source, size_t nelems, int PE_st
                       int logPE_stride, int PE_size, long *pSync);
 void shmem_fcollect64(void *target, const void *source, size_t nelems, int PE_start,
                       int logPE_stride, int PE_size, long *pSync);
+void shmem_collect32(void *target, const void *source, size_t nelems, int PE_start,
+                     int logPE_stride, int PE_size, long *pSync);
+void shmem_collect64(void *target, const void *source, size_t nelems, int PE_start,
+                     int logPE_stride, int PE_size, long *pSync);
 void shmem_alltoall32(void *target, const void *source, size_t nelems, int PE_start,
                       int logPE_stride, int PE_size, long *pSync);
 void shmem_alltoall64(void *target, const void *source, size_t nelems, int PE_start,

@@ -107,6 +107,19 @@ class Restatement:
         self.L.or_fcollect(P, x[0].nbytes, _ptr(x), _ptr(out))
         return out
 
+    def collect(self, x, nbytes, dest_bytes):
+        """x: [P, >= max(nbytes)] uint8 rows; member k contributes nbytes[k];
+        returns [P, dest_bytes] uint8 with the concatenation first."""
+        x = np.ascontiguousarray(x, dtype=np.uint8)
+        P = x.shape[0]
+        nb = np.ascontiguousarray(nbytes, dtype=np.uint64)
+        out = np.zeros((P, dest_bytes), dtype=np.uint8)
+        rc = self.L.or_collect(P, _ptr(nb), _ptr(x), ctypes.c_size_t(x.shape[1]), _ptr(out),
+                               ctypes.c_size_t(dest_bytes))
+        if rc != 0:
+            raise ValueError("oracle collect rejected its sizes")
+        return out
+
     def alltoall(self, x):
         """x: [P, P*n]: row k is member k's source (P blocks)."""
         x = np.ascontiguousarray(x)
@@ -150,7 +163,8 @@ def _dtype_name(dt):
 
 # job kinds understood by ref_run (oracle/ref_harness/pe_emu.c)
 K_REDUCE_TEAM, K_TO_ALL, K_SIZED, K_TEAM_COPY, K_ALLTOALLS_SIZED, K_ALLTOALLS_TEAM, \
-    K_BARRIER, K_BARRIER_ALL, K_TEAM_SYNC, K_BROADCAST_SIZED, K_BROADCAST_TEAM = range(11)
+    K_BARRIER, K_BARRIER_ALL, K_TEAM_SYNC, K_BROADCAST_SIZED, K_BROADCAST_TEAM, \
+    K_COLLECT_SIZED, K_COLLECT_TEAM = range(13)
 
 
 class Reference:

@@ -224,7 +224,13 @@ enum ref_kind {
   REF_BROADCAST_SIZED = 9, /* void f(void*, const void*, size_t, int root,
                               int, int, int, long*)                          */
   REF_BROADCAST_TEAM = 10, /* int f(team, T*, const T*, size_t, int root)     */
+  REF_COLLECT_SIZED = 11,  /* void f(void*, const void*, size_t, int,int,int,long*)
+                              with each member's own count (below)           */
+  REF_COLLECT_TEAM = 12,   /* int f(team, void*, const void*, size_t), own count */
 };
+
+struct ref_job;
+static size_t collect_count(const struct ref_job *j, int as);
 
 struct ref_job {
   int kind;
@@ -241,6 +247,13 @@ struct ref_job {
   pthread_barrier_t bar;
   int pin;
 };
+
+/* Collect takes a different count on every member: member i passes
+ * nelems + (i * a) % (b + 1) (a rule the caller knows, so it can size and
+ * check the result). */
+static size_t collect_count(const struct ref_job *j, int as) {
+  return j->nelems + (size_t)(((long)as * j->a) % (j->b + 1));
+}
 
 static int member_index(const struct ref_job *j, int pe) {
   const int stride = 1 << j->log_stride;
@@ -299,6 +312,15 @@ static void call_once(struct ref_job *j, char *src, char *dst, long *psync) {
   case REF_BROADCAST_TEAM:
     ((int (*)(shmem_team_t, void *, const void *, size_t, int))j->fn)(
         team, dst, src, j->nelems, (int)j->a);
+    break;
+  case REF_COLLECT_SIZED:
+    ((void (*)(void *, const void *, size_t, int, int, int, long *))j->fn)(
+        dst, src, collect_count(j, member_index(j, t_me)), j->pe_start, stride_log,
+        j->pe_size, psync);
+    break;
+  case REF_COLLECT_TEAM:
+    ((int (*)(shmem_team_t, void *, const void *, size_t))j->fn)(
+        team, dst, src, collect_count(j, member_index(j, t_me)));
     break;
   default:
     emu_die("unknown job kind");

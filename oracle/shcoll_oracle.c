@@ -308,6 +308,32 @@ int or_fcollect(int npes, size_t nbytes, const void *in, void *out) {
   return 0;
 }
 
+/* collect.c:35-591: every member contributes its own nbytes[k]; member p's
+ * dest is the contributions concatenated in member order (each member's
+ * block offset is the exclusive prefix sum of the sizes, collect.c:43,
+ * util/scan.c:10).  in: member k's source starts at in + k*src_pitch;
+ * out: member p's dest starts at out + p*dst_pitch. */
+int or_collect(int npes, const uint64_t *nbytes, const void *in, size_t src_pitch, void *out,
+               size_t dst_pitch) {
+  if (npes < 1) return -1;
+  const char *src = (const char *)in;
+  char *dst = (char *)out;
+  size_t total = 0;
+  for (int k = 0; k < npes; k++) {
+    if (nbytes[k] > src_pitch) return -1;
+    total += nbytes[k];
+  }
+  if (total > dst_pitch) return -1;
+  for (int p = 0; p < npes; p++) {
+    size_t off = 0;
+    for (int k = 0; k < npes; k++) {
+      memcpy(dst + (size_t)p * dst_pitch + off, src + (size_t)k * src_pitch, nbytes[k]);
+      off += nbytes[k];
+    }
+  }
+  return 0;
+}
+
 /* alltoall.c:75-201: block k of member j's dest is block j of member k's
  * source. */
 int or_alltoall(int npes, size_t nbytes, const void *in, void *out) {

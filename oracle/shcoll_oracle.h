@@ -36,6 +36,8 @@ int or_reduce(int algo, int op, int dtype, int npes, size_t nelems,
 size_t or_dtype_size(int dtype);
 
 int or_fcollect(int npes, size_t nbytes, const void *in, void *out);
+int or_collect(int npes, const uint64_t *nbytes, const void *in, size_t src_pitch, void *out,
+               size_t dst_pitch);
 int or_alltoall(int npes, size_t nbytes, const void *in, void *out);
 int or_alltoalls(int npes, size_t nelems, long dst, long sst, size_t esize,
                  const void *in, void *out);

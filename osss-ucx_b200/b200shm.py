@@ -65,6 +65,7 @@ def _load():
         "b200shm_reduce_host": (ci, [ci, ci, ci, ci, ci, ci, vp, u64, vp, u64, u64, u64, u64, vp]),
         "b200shm_fcollect": (ci, [ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_alltoall": (ci, [ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_collect": (ci, [ci, ci, ci, u64, u64, vp, vp]),
         "b200shm_alltoalls": (ci, [ci, ci, ci, u64, u64, i64, i64, u64, u64, vp]),
         "b200shm_broadcast": (ci, [ci, ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_barrier": (ci, [ci, ci, ci, ci, vp]),
@@ -205,6 +206,15 @@ def reduce_noalloc(op, dtype, algo, npes, dest_ptr, dest_stride, src_ptr, src_st
 def fcollect(dest, src, nbytes, team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_fcollect(start, stride, size, dest, src, nbytes, stream))
+
+
+def collect(dest, src, nbytes, team=None, stream=None):
+    """Variable-size allgather: member k contributes nbytes[k] bytes."""
+    start, stride, size = _team(team)
+    nb = np.ascontiguousarray(nbytes, dtype=np.uint64)
+    if len(nb) != size:
+        raise ValueError("one size per member")
+    return _check(lib.b200shm_collect(start, stride, size, dest, src, nb.ctypes.data, stream))
 
 
 def alltoall(dest, src, nbytes, team=None, stream=None):

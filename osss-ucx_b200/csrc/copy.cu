@@ -1,6 +1,6 @@
 /*
- * copy.cu -- the data-movement collectives: fcollect, alltoall, strided
- * alltoall and broadcast.
+ * copy.cu -- the data-movement collectives: fcollect, collect, alltoall,
+ * strided alltoall and broadcast.
  *
  * In the reference every byte crosses a process boundary as a UCX put
  * (fcollect: log2(P) Bruck rounds plus an in-place byte rotation,
@@ -15,6 +15,8 @@
  * multiple of 16, else in bytes (or elements for the strided form).
  */
 #include <stdint.h>
+
+#include <vector>
 
 #include "internal.cuh"
 
@@ -53,6 +55,26 @@ __global__ void __launch_bounds__(256) k_fcollect(const char *src0, char *dst0, 
       const char c = src[v];
       for (int j = 0; j < P; j++) dst[(uint64_t)j * step + v] = c;
     }
+  }
+}
+
+/* collect: member k contributes sizes[k] bytes; member j's
+ * dest[prefix[k] + b] = member k's src[b] (collect.c:35-591: the
+ * contributions concatenated in member order).  blockIdx.y = source member
+ * k; each thread reads one word of k's contribution once and writes it
+ * into every member's dest.  W is a width every offset and size divides. */
+template <class W>
+__global__ void __launch_bounds__(256) k_collect(const char *src0, char *dst0, uint64_t step,
+                                                 int P, const uint64_t *sizes,
+                                                 const uint64_t *prefix) {
+  const int k = blockIdx.y;
+  const W *src = (const W *)(src0 + (uint64_t)k * step);
+  char *dst = dst0 + prefix[k];
+  const uint64_t n = sizes[k] / sizeof(W);
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const W u = src[v];
+    for (int j = 0; j < P; j++) ((W *)(dst + (uint64_t)j * step))[v] = u;
   }
 }
 
@@ -165,6 +187,49 @@ int fcollect_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint6
   return B200SHM_OK;
 }
 
+int collect_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint64_t src_off,
+                   const uint64_t *nbytes, cudaStream_t s) {
+  int rc = check_team(pe_start, pe_stride, P);
+  if (rc) return rc;
+  if (!nbytes) return fail(B200SHM_ERR_ARG, "collect: null size array");
+  if (P > 65535) return fail(B200SHM_ERR_UNSUPPORTED, "collect: more than 65535 members");
+  std::vector<uint64_t> host(2 * (size_t)P);
+  uint64_t total = 0, biggest = 0, bits = 0;
+  for (int k = 0; k < P; k++) {
+    if (nbytes[k] > st().slice || total + nbytes[k] > st().slice)
+      return fail(B200SHM_ERR_ARG, "collect: contributions larger than a heap slice");
+    host[k] = nbytes[k];
+    host[P + k] = total;
+    total += nbytes[k];
+    if (nbytes[k] > biggest) biggest = nbytes[k];
+    bits |= nbytes[k];
+  }
+  if ((rc = check_extent(src_off, biggest, "collect source"))) return rc;
+  if ((rc = check_extent(dest_off, total, "collect dest"))) return rc;
+  if (overlaps(dest_off, total, src_off, biggest))
+    return fail(B200SHM_ERR_ARG, "collect: dest and source overlap");
+  if (total == 0) return B200SHM_OK;
+  Members m = members(pe_start, pe_stride, P);
+  bits |= src_off | dest_off | m.step;
+  const uint64_t w = bits & 15 ? (bits & 7 ? (bits & 3 ? 1 : 4) : 8) : 16;
+  uint64_t *dev = nullptr;
+  B200_CK(cudaMallocAsync((void **)&dev, host.size() * sizeof(uint64_t), s));
+  B200_CK(cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(uint64_t),
+                          cudaMemcpyHostToDevice, s));
+  dim3 grid(x_blocks(biggest / w, P, 8ull * st().sm_count * 4), P);
+  const char *src = m.first + src_off;
+  char *dst = m.first + dest_off;
+  switch (w) {
+  case 16: k_collect<uint4><<<grid, 256, 0, s>>>(src, dst, m.step, P, dev, dev + P); break;
+  case 8: k_collect<unsigned long long><<<grid, 256, 0, s>>>(src, dst, m.step, P, dev, dev + P); break;
+  case 4: k_collect<unsigned><<<grid, 256, 0, s>>>(src, dst, m.step, P, dev, dev + P); break;
+  default: k_collect<unsigned char><<<grid, 256, 0, s>>>(src, dst, m.step, P, dev, dev + P); break;
+  }
+  count_launch();
+  B200_CK(cudaFreeAsync(dev, s));
+  return B200SHM_OK;
+}
+
 int alltoall_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint64_t src_off,
                     uint64_t B, cudaStream_t s) {
   int rc = check_team(pe_start, pe_stride, P);
@@ -268,6 +333,13 @@ int b200shm_fcollect(int pe_start, int pe_stride, int pe_size, uint64_t dest_off
   int rc = fcollect_launch(pe_start, pe_stride, pe_size, dest_off, src_off, nbytes,
                            pick_stream(stream));
   return rc ? rc : finish(stream, "b200shm_fcollect");
+}
+
+int b200shm_collect(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,
+                    uint64_t src_off, const uint64_t *nbytes, void *stream) {
+  int rc = collect_launch(pe_start, pe_stride, pe_size, dest_off, src_off, nbytes,
+                          pick_stream(stream));
+  return rc ? rc : finish(stream, "b200shm_collect");
 }
 
 int b200shm_alltoall(int pe_start, int pe_stride, int pe_size, uint64_t dest_off,

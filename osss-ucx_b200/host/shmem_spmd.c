@@ -69,7 +69,7 @@ static __thread int t_pe = -1;
 
 /* ---- arrival points ----------------------------------------------------- */
 enum { K_NONE, K_MALLOC, K_FREE, K_BARRIER, K_REDUCE, K_FCOLLECT, K_ALLTOALL, K_ALLTOALLS,
-       K_BROADCAST, K_SPLIT, K_SPLIT2D, K_DESTROY };
+       K_BROADCAST, K_SPLIT, K_SPLIT2D, K_DESTROY, K_COLLECT };
 
 typedef struct coll {
   int kind, op, dtype, algo, root;
@@ -85,6 +85,8 @@ typedef struct agg {
   coll_t req;
   uint64_t out;
   void *outp, *outq;
+  uint64_t *counts; /* collect: each member's own byte count, by team index */
+  int counts_cap;
 } agg_t;
 
 typedef struct b200_team {
@@ -158,9 +160,11 @@ static b200_team_t *active_set(int start, int logstride, int size) {
 }
 
 static int same_req(const coll_t *x, const coll_t *y) {
+  /* collect is the one collective whose count differs between members */
   return x->kind == y->kind && x->op == y->op && x->dtype == y->dtype && x->algo == y->algo &&
-         x->root == y->root && x->dest == y->dest && x->src == y->src && x->n == y->n &&
-         x->esize == y->esize && x->a == y->a && x->b == y->b;
+         x->root == y->root && x->dest == y->dest && x->src == y->src &&
+         (x->n == y->n || x->kind == K_COLLECT) && x->esize == y->esize && x->a == y->a &&
+         x->b == y->b;
 }
 
 static int launch(b200_team_t *t, agg_t *g);
@@ -179,6 +183,17 @@ static int arrive(b200_team_t *t, const coll_t *mine) {
     g->mismatch = 0;
   } else if (!same_req(&g->req, mine)) {
     g->mismatch = 1;
+  }
+  if (mine->kind == K_COLLECT) {
+    if (g->counts_cap < t->size) {
+      uint64_t *c = (uint64_t *)realloc(g->counts, (size_t)t->size * sizeof(uint64_t));
+      if (!c) g->mismatch = 1;
+      else {
+        g->counts = c;
+        g->counts_cap = t->size;
+      }
+    }
+    if (g->counts_cap >= t->size) g->counts[team_index(t, t_pe)] = mine->n;
   }
   if (++g->arrived == t->size) {
     g->rc = g->mismatch ? set_err(B200SHM_ERR_ARG,
@@ -253,6 +268,9 @@ static int launch(b200_team_t *t, agg_t *g) {
     return engine_err(b200shm_fcollect(t->start, t->stride, t->size, r->dest, r->src, r->n, NULL));
   case K_ALLTOALL:
     return engine_err(b200shm_alltoall(t->start, t->stride, t->size, r->dest, r->src, r->n, NULL));
+  case K_COLLECT:
+    return engine_err(b200shm_collect(t->start, t->stride, t->size, r->dest, r->src, g->counts,
+                                      NULL));
   case K_ALLTOALLS:
     return engine_err(b200shm_alltoalls(t->start, t->stride, t->size, r->dest, r->src, r->a, r->b,
                                         r->n, r->esize, NULL));
@@ -634,6 +652,11 @@ static int copy_on(b200_team_t *t, int kind, void *dest, const void *source, uin
     return copy_on((b200_team_t *)team, K_FCOLLECT, dest, source,              \
                    nelems * sizeof(_type), 0, 0, 0, 0);                        \
   }                                                                            \
+  int shmem_##_tn##_collect(shmem_team_t team, _type *dest,                   \
+                            const _type *source, size_t nelems) {             \
+    return copy_on((b200_team_t *)team, K_COLLECT, dest, source,               \
+                   nelems * sizeof(_type), 0, 0, 0, 0);                        \
+  }                                                                            \
   int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                  \
                              const _type *source, size_t nelems) {            \
     return copy_on((b200_team_t *)team, K_ALLTOALL, dest, source,              \
@@ -656,6 +679,9 @@ SHMEM_B200_RMA_TYPES(DEF_COPY)
 int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems) {
   return copy_on((b200_team_t *)team, K_FCOLLECT, dest, source, nelems, 0, 0, 0, 0);
 }
+int shmem_collectmem(shmem_team_t team, void *dest, const void *source, size_t nelems) {
+  return copy_on((b200_team_t *)team, K_COLLECT, dest, source, nelems, 0, 0, 0, 0);
+}
 int shmem_alltoallmem(shmem_team_t team, void *dest, const void *source, size_t nelems) {
   return copy_on((b200_team_t *)team, K_ALLTOALL, dest, source, nelems, 0, 0, 0, 0);
 }
@@ -675,6 +701,13 @@ int shmem_broadcastmem(shmem_team_t team, void *dest, const void *source, size_t
                              long *pSync) {                                    \
     (void)pSync;                                                               \
     copy_on(active_set(PE_start, logPE_stride, PE_size), K_FCOLLECT, target,   \
+            source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
+  }                                                                            \
+  void shmem_collect##_bits(void *target, const void *source, size_t nelems,  \
+                            int PE_start, int logPE_stride, int PE_size,       \
+                            long *pSync) {                                     \
+    (void)pSync;                                                               \
+    copy_on(active_set(PE_start, logPE_stride, PE_size), K_COLLECT, target,    \
             source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
   }                                                                            \
   void shmem_alltoall##_bits(void *target, const void *source, size_t nelems, \

@@ -133,3 +133,37 @@ def test_copy_argument_errors(B, heap):
         B.alltoalls(a, a + 512, 0, 1, 4, 8, team=(0, 1, 2))  # zero stride
     with pytest.raises(B.B200Error):
         B.broadcast(9, a, a + 512, 64, team=(0, 1, 4))  # root not a member
+
+
+@pytest.mark.parametrize("team,counts,align", [
+    ((0, 1, 4), [16, 32, 0, 48], 16),          # 16-byte words, one member empty
+    ((3, 2, 5), [8, 24, 40, 8, 16], 8),        # 8-byte words, strided team
+    ((10, 3, 6), [12, 4, 28, 20, 0, 8], 4),    # 4-byte words
+    ((0, 1, 7), [3, 1, 5, 7, 2, 9, 4], 1),     # bytes
+    ((255, 1, 1), [1000], 8),                  # one member
+])
+def test_collect_matches_oracle(B, heap, rs, team, counts, align):
+    """Variable-size allgather: member k contributes counts[k] bytes; every
+    member's dest holds the contributions concatenated in member order."""
+    P = team[2]
+    rng = np.random.default_rng(sum(counts) + P)
+    src_bytes = max(max(counts), 16)
+    x = rng.integers(0, 256, (P, src_bytes), dtype=np.uint8)
+    total = sum(counts)
+    s = heap(src_bytes + 64) + (align if align < 16 else 0)
+    d = heap(total + 64) + (align if align < 16 else 0)
+    B.put_rows(s, x, team=team)
+    B.memset(d, 0x77, total + 16, team=team)
+    B.collect(d, s, counts, team=team)
+    got = B.get_rows(d, total + 16, np.uint8, team=team)
+    want = rs.collect(x, counts, total + 16)
+    want[:, total:] = 0x77
+    assert got.tobytes() == want.tobytes()
+
+
+def test_collect_rejects_bad_arguments(B, heap):
+    a = heap(4096)
+    with pytest.raises(B.B200Error):
+        B.collect(a, a + 64, [64, 64, 64], team=(0, 1, 3))  # dest overlaps source
+    with pytest.raises(ValueError):
+        B.collect(a, a + 2048, [8, 8], team=(0, 1, 3))      # one size per member

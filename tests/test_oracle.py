@@ -174,3 +174,40 @@ def test_restatement_matches_reference_copies(rs, ref):
                             nelems=n, a=dst, b=sst)
                     got = rs.alltoalls(x, d0, dst, sst, n)
                     assert got.tobytes() == out.tobytes(), (base, sync, P, dst, sst)
+
+
+COLLECT_ALGOS = ["linear", "all_linear", "all_linear1", "rec_dbl", "rec_dbl_signal", "ring",
+                 "bruck", "bruck_no_rotate"]
+
+
+@pytest.mark.parametrize("algo", COLLECT_ALGOS)
+def test_restatement_matches_reference_collect(rs, ref, algo):
+    """Collect with a different count on every member (member i passes
+    base + (i*a) % (b+1), the rule the emulator applies): the reference's
+    sized (32/64) and team (typed, mem) forms against the restatement.
+    collect_helper_simple is left out: it copies each PE's block into its own
+    dest only (collect.c:35-52), so it exchanges no data; so is linear over a
+    single PE, which adds to PE me + stride outside the set (collect.c:80)."""
+    rng = np.random.default_rng(17)
+    sizes = (1, 2, 4, 8) if algo.startswith("rec_dbl") else (1, 2, 3, 5, 8)
+    if algo == "linear":
+        sizes = sizes[1:]
+    for P in sizes:
+        for base, a, b in ((3, 5, 6), (0, 2, 3), (11, 1, 1)):
+            counts = [base + (i * a) % (b + 1) for i in range(P)]
+            for es, tag in ((4, "collect32"), (8, "collect64")):
+                x = rng.integers(0, 256, size=(P, max(max(counts) * es, 1)), dtype=np.uint8)
+                tot = sum(counts) * es
+                out = np.zeros((P, tot + 16), np.uint8)
+                ref.run(oracle.K_COLLECT_SIZED, f"shcoll_{tag}_{algo}", x, out, nelems=base, a=a,
+                        b=b)
+                want = rs.collect(x, [c * es for c in counts], tot + 16)
+                assert out.tobytes() == want.tobytes(), (algo, P, base, a, b, es)
+            if algo.startswith("rec_dbl"):
+                continue
+            x = rng.integers(0, 256, size=(P, max(max(counts) * 8, 1)), dtype=np.uint8)
+            out = np.zeros((P, sum(counts) * 8 + 8), np.uint8)
+            ref.run(oracle.K_COLLECT_TEAM, f"shcoll_int64_collect_{algo}", x, out, nelems=base,
+                    a=a, b=b)
+            want = rs.collect(x, [c * 8 for c in counts], sum(counts) * 8 + 8)
+            assert out.tobytes() == want.tobytes(), (algo, P, "team")

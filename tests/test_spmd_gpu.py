@@ -89,3 +89,46 @@ def test_spmd_program_matches_oracle(tmp_path, rs):
             assert info[pe][0] == -1 and info[pe][1] == -1
         assert info[pe][2] == (pe % 4) * 100 + 4
         assert info[pe][3] == (pe // 4) * 100 + 2
+
+
+NC = 6
+OUTC = np.dtype([("c32", np.int32, (NC, 3 * NC * (NC + 1) // 2)), ("c64", np.int64, (NC, 15)),
+                 ("cm", np.uint8, (NC, 5 * NC + NC * (NC - 1) // 2)), ("status", np.int32, (NC,))],
+                align=True)
+
+
+@pytest.mark.gpu
+def test_spmd_collect_matches_oracle(tmp_path, rs):
+    """shmem_int32_collect (team), shmem_collect64 (active set of the even
+    PEs) and shmem_collectmem, each PE passing its own count."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_collect")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_collect.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([exe, str(outp)], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    o = np.fromfile(outp, dtype=OUTC)[0]
+    assert (o["status"] == 0).all()
+    c32 = [3 * (i + 1) for i in range(NC)]
+    x = np.zeros((NC, max(c32)), np.int32)
+    for i in range(NC):
+        x[i, :c32[i]] = i * 1000 + np.arange(c32[i])
+    want = rs.collect(x.view(np.uint8), [c * 4 for c in c32], sum(c32) * 4)
+    assert o["c32"].tobytes() == want.tobytes()
+    evens = [0, 2, 4]
+    c64 = [2 * i + 1 for i in evens]
+    x = np.zeros((3, max(c64)), np.int64)
+    for k, i in enumerate(evens):
+        x[k, :c64[k]] = (i << 40) | np.arange(c64[k])
+    want = rs.collect(x.view(np.uint8), [c * 8 for c in c64], sum(c64) * 8)
+    assert o["c64"][evens].tobytes() == want.tobytes()
+    assert (o["c64"][1::2] == 0).all()
+    cm = [5 + i for i in range(NC)]
+    x = np.zeros((NC, max(cm)), np.uint8)
+    for i in range(NC):
+        x[i, :cm[i]] = (i * 16 + np.arange(cm[i])) & 0xFF
+    assert o["cm"].tobytes() == rs.collect(x, cm, sum(cm)).tobytes()
