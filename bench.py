@@ -195,6 +195,22 @@ def run_reference_arm(args, rank):
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
+def max_over_ranks(ms, dist, device):
+    """The job's time for a step: the slowest rank's (every rank runs its
+    own team on its own GPU, so the job is done when the last one is)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbs(bytes_per_rank_step, steps, world, ms):
+    """Whole-job throughput: the bytes all ranks moved over the job's time."""
+    return bytes_per_rank_step * steps * world / (ms / 1e3) / 1e9
+
+
 def main():
     global N
     ap = argparse.ArgumentParser()
@@ -304,12 +320,8 @@ def main():
     launches = B.launch_count() - launches0
     clk = clocks.stop()
     barrier()
-    ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = step_bytes * args.steps * world / (ms / 1e3) / 1e9
+    ms = max_over_ranks(start.elapsed_time(end), dist, "cuda")
+    value = job_gbs(step_bytes, args.steps, world, ms)
 
     # per-kernel durations (the reduce kernel of each (dtype, op, order))
     durs = {}
@@ -358,12 +370,8 @@ def main():
         e1.record(s)
         B.quiet()
         barrier()
-        ems = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": round(step_bytes * args.e2e_steps * world / (ems / 1e3) / 1e9, 3),
+        ems = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+        e2e = {"value": round(job_gbs(step_bytes, args.e2e_steps, world, ems), 3),
                "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "steps": args.e2e_steps, "ms_per_step": round(ems / args.e2e_steps, 3),
                "path": "b200shm_reduce_host (pinned host rows in and out; copy in, reduce and "
