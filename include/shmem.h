@@ -203,7 +203,11 @@ SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_PROD)
   void shmem_##_tn##_get(_type *dest, const _type *source, size_t nelems,      \
                          int pe);                                               \
   void shmem_##_tn##_p(_type *dest, _type value, int pe);                      \
-  _type shmem_##_tn##_g(const _type *source, int pe);
+  _type shmem_##_tn##_g(const _type *source, int pe);                          \
+  void shmem_##_tn##_put_nbi(_type *dest, const _type *source, size_t nelems,  \
+                             int pe);                                           \
+  void shmem_##_tn##_get_nbi(_type *dest, const _type *source, size_t nelems,  \
+                             int pe);
 SHMEM_B200_RMA_TYPES(SHMEM_B200_DECL_COPY)
 int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
 /* collect: each PE passes its own nelems; dest gets the contributions
@@ -272,6 +276,31 @@ void shmem_broadcast64(void *target, const void *source, size_t nelems, int PE_r
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
+
+/* Non-blocking fetching atomics (api.h: shmem_<T>_atomic_fetch_add_nbi and
+ * the family): *fetch holds the old value after the next shmem_quiet or
+ * barrier.  They and the _nbi puts/gets between symmetric objects run
+ * through the engine's serving loop. */
+#define SHMEM_B200_DECL_AMO_NBI_STD(_type, _tn)                                 \
+  void shmem_##_tn##_atomic_fetch_add_nbi(_type *fetch, _type *dest,           \
+                                          _type value, int pe);                 \
+  void shmem_##_tn##_atomic_fetch_inc_nbi(_type *fetch, _type *dest, int pe);  \
+  void shmem_##_tn##_atomic_compare_swap_nbi(_type *fetch, _type *dest,        \
+                                             _type cond, _type value, int pe);
+#define SHMEM_B200_DECL_AMO_NBI_EXT(_type, _tn)                                 \
+  void shmem_##_tn##_atomic_swap_nbi(_type *fetch, _type *dest, _type value,   \
+                                     int pe);                                   \
+  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source, int pe);
+#define SHMEM_B200_DECL_AMO_NBI_BIT(_type, _tn)                                 \
+  void shmem_##_tn##_atomic_fetch_and_nbi(_type *fetch, _type *dest,           \
+                                          _type value, int pe);                 \
+  void shmem_##_tn##_atomic_fetch_or_nbi(_type *fetch, _type *dest,            \
+                                         _type value, int pe);                  \
+  void shmem_##_tn##_atomic_fetch_xor_nbi(_type *fetch, _type *dest,           \
+                                          _type value, int pe);
+SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_NBI_STD)
+SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_NBI_EXT)
+SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_NBI_BIT)
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,7 @@
  */
 #include <errno.h>
 #include <pthread.h>
+#include <sched.h>
 #include <stdarg.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -374,6 +375,8 @@ static void *pe_trampoline(void *p) {
   return NULL;
 }
 
+static void stop_job_server(void);
+
 int shmemx_b200_run(int npes, void (*pe_main)(void *), void *arg) {
   if (npes < 1 || !pe_main) return set_err(B200SHM_ERR_ARG, "shmemx_b200_run: bad arguments");
   int rc = engine_up(npes);
@@ -391,6 +394,7 @@ int shmemx_b200_run(int npes, void (*pe_main)(void *), void *arg) {
   for (int p = 0; p < npes; p++) pthread_join(th[p], NULL);
   free(th);
   free(args);
+  stop_job_server();
   return 0;
 }
 
@@ -443,6 +447,129 @@ void *shmem_ptr(const void *dest, int pe) {
 }
 
 /* ---- RMA ----------------------------------------------------------------------- */
+/* ---- non-blocking operations: the serving loop ------------------------------ */
+/* A _nbi put/get between two symmetric objects, and a fetching _nbi atomic,
+ * is a request to the job's serving loop (b200shm_serve_*, started by the
+ * first such call); the PE thread keeps its tickets, and shmem_quiet (and
+ * every barrier, which implies quiet) waits for them and writes the fetched
+ * values.  A put or get whose local buffer is not symmetric takes the
+ * blocking path, which is complete on return as well. */
+static pthread_mutex_t g_srv_mu = PTHREAD_MUTEX_INITIALIZER;
+static b200shm_server *g_srv;
+typedef struct {
+  uint64_t ticket;
+  void *fetch;
+  int size;
+} nbi_t;
+static __thread nbi_t *t_nbi;
+static __thread int t_nbi_n, t_nbi_cap;
+
+static b200shm_server *job_server(void) {
+  pthread_mutex_lock(&g_srv_mu);
+  if (!g_srv && b200shm_serve_start(4096, 0, 1.0, &g_srv) != 0) g_srv = NULL;
+  b200shm_server *s = g_srv;
+  pthread_mutex_unlock(&g_srv_mu);
+  return s;
+}
+
+static void stop_job_server(void) {
+  pthread_mutex_lock(&g_srv_mu);
+  if (g_srv) b200shm_serve_stop(g_srv);
+  g_srv = NULL;
+  pthread_mutex_unlock(&g_srv_mu);
+}
+
+/* Complete this PE's outstanding requests. */
+static int nbi_quiet(void) {
+  int rc = 0;
+  for (int i = 0; i < t_nbi_n; i++) {
+    uint64_t f = 0;
+    const int r = b200shm_serve_wait(g_srv, t_nbi[i].ticket, 60.0, &f);
+    if (r) rc = engine_err(r);
+    else if (t_nbi[i].fetch) memcpy(t_nbi[i].fetch, &f, (size_t)t_nbi[i].size);
+  }
+  t_nbi_n = 0;
+  return rc;
+}
+
+/* 0 when queued, 1 when the loop is unavailable (take the blocking path), <0 on error. */
+static int nbi_enqueue(const b200shm_request *r, void *fetch, int size) {
+  b200shm_server *s = job_server();
+  if (!s) return 1;
+  uint64_t tk = 0;
+  const double t0 = shmemx_wtime();
+  for (;;) {
+    const int rc = b200shm_serve_enqueue(s, r, &tk);
+    if (rc == 0) break;
+    if (rc != B200SHM_ERR_BUSY) return engine_err(rc);
+    if (t_nbi_n) nbi_quiet(); /* free slots held by this PE */
+    else sched_yield();       /* slots held by other PEs free as the GPU completes them */
+    if (shmemx_wtime() - t0 > 60.0) return set_err(B200SHM_ERR_TIMEOUT, "nbi: no free slot");
+  }
+  if (t_nbi_n == t_nbi_cap) {
+    const int cap = t_nbi_cap ? 2 * t_nbi_cap : 64;
+    nbi_t *n = (nbi_t *)realloc(t_nbi, (size_t)cap * sizeof(nbi_t));
+    if (!n) {
+      uint64_t f = 0;
+      b200shm_serve_wait(s, tk, 60.0, &f);
+      if (fetch) memcpy(fetch, &f, (size_t)size);
+      return 0;
+    }
+    t_nbi = n;
+    t_nbi_cap = cap;
+  }
+  t_nbi[t_nbi_n].ticket = tk;
+  t_nbi[t_nbi_n].fetch = fetch;
+  t_nbi[t_nbi_n].size = size;
+  t_nbi_n++;
+  return 0;
+}
+
+/* put (kind PUT) or get (kind GET) of n bytes between this PE and `pe`; 1 if
+ * an address is not symmetric */
+static int nbi_rma(int kind, void *dest, const void *source, size_t n, int pe) {
+  uint64_t doff, soff;
+  const char *mine = g_base + (uint64_t)t_pe * g_slice;
+  const char *d = (const char *)dest, *sp = (const char *)source;
+  if (d < mine || d >= mine + g_slice || sp < mine || sp >= mine + g_slice) return 1;
+  doff = (uint64_t)(d - mine);
+  soff = (uint64_t)(sp - mine);
+  b200shm_request r;
+  memset(&r, 0, sizeof(r));
+  r.kind = kind;
+  r.pe_start = t_pe;
+  r.pe_stride = 1;
+  r.pe_size = 1;
+  r.pe = pe;
+  r.dest_off = doff;
+  r.src_off = soff;
+  r.n = n;
+  return nbi_enqueue(&r, NULL, 0);
+}
+
+static void nbi_amo(int op, int dtype, const void *dest, int pe, const void *value,
+                    const void *cond, void *fetch, int size) {
+  uint64_t off;
+  if (sym_off(dest, &off)) {
+    t_status = B200SHM_ERR_ARG;
+    return;
+  }
+  b200shm_request r;
+  memset(&r, 0, sizeof(r));
+  r.kind = B200SHM_REQ_AMO;
+  r.op = op;
+  r.dtype = dtype;
+  r.pe = pe;
+  r.dest_off = off;
+  if (value) memcpy(&r.value, value, (size_t)size);
+  if (cond) memcpy(&r.cond, cond, (size_t)size);
+  const int rc = nbi_enqueue(&r, fetch, size);
+  if (rc == 1) /* no serving loop: the blocking form */
+    t_status = engine_err(b200shm_amo(op, dtype, pe, off, value, cond, fetch));
+  else
+    t_status = rc;
+}
+
 void shmem_putmem(void *dest, const void *source, size_t nelems, int pe) {
   uint64_t off;
   if (sym_off(dest, &off) == 0) t_status = engine_err(b200shm_memcpy(b200shm_ptr(pe, off), source, nelems, NULL));
@@ -452,13 +579,23 @@ void shmem_getmem(void *dest, const void *source, size_t nelems, int pe) {
   if (sym_off(source, &off) == 0) t_status = engine_err(b200shm_memcpy(dest, b200shm_ptr(pe, off), nelems, NULL));
 }
 void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
-  shmem_putmem(dest, source, nelems, pe);
+  const int rc = nbi_rma(B200SHM_REQ_PUT, dest, source, nelems, pe);
+  if (rc == 1) shmem_putmem(dest, source, nelems, pe);
+  else t_status = rc;
 }
 void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
-  shmem_getmem(dest, source, nelems, pe);
+  const int rc = nbi_rma(B200SHM_REQ_GET, dest, source, nelems, pe);
+  if (rc == 1) shmem_getmem(dest, source, nelems, pe);
+  else t_status = rc;
 }
-void shmem_fence(void) { b200shm_quiet(); }
-void shmem_quiet(void) { b200shm_quiet(); }
+/* Requests in flight may complete in any order, so fence (ordering of this
+ * PE's puts to one PE) is as strong as quiet here. */
+void shmem_fence(void) { shmem_quiet(); }
+void shmem_quiet(void) {
+  int rc = t_nbi_n ? nbi_quiet() : 0;
+  const int r2 = b200shm_quiet();
+  t_status = rc ? rc : engine_err(r2);
+}
 
 #define DEF_RMA(_type, _tn)                                                    \
   void shmem_##_tn##_put(_type *dest, const _type *source, size_t nelems,     \
@@ -477,11 +614,20 @@ void shmem_quiet(void) { b200shm_quiet(); }
     memset(&v, 0, sizeof(v));                                                  \
     shmem_getmem(&v, source, sizeof(_type), pe);                               \
     return v;                                                                  \
+  }                                                                            \
+  void shmem_##_tn##_put_nbi(_type *dest, const _type *source, size_t nelems, \
+                             int pe) {                                         \
+    shmem_putmem_nbi(dest, source, nelems * sizeof(_type), pe);                \
+  }                                                                            \
+  void shmem_##_tn##_get_nbi(_type *dest, const _type *source, size_t nelems, \
+                             int pe) {                                         \
+    shmem_getmem_nbi(dest, source, nelems * sizeof(_type), pe);                \
   }
 SHMEM_B200_RMA_TYPES(DEF_RMA)
 
 /* ---- synchronisation ---------------------------------------------------------- */
 static int barrier_on(b200_team_t *t, int algo) {
+  if (t_nbi_n) nbi_quiet(); /* a barrier completes this PE's outstanding requests */
   coll_t r = {0};
   r.kind = K_BARRIER;
   r.algo = algo;
@@ -857,3 +1003,51 @@ static void amo(int op, int dtype, const void *dest, int pe, const void *value, 
 SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_BIT)
+
+/* the fetching atomics' _nbi forms: the old value lands in *fetch at quiet */
+#define DEF_AMO_NBI_STD(_type, _tn)                                            \
+  void shmem_##_tn##_atomic_fetch_add_nbi(_type *fetch, _type *dest,          \
+                                          _type value, int pe) {               \
+    nbi_amo(B200SHM_AMO_FETCH_ADD, B200_DTYPE_OF(_type), dest, pe, &value,     \
+            NULL, fetch, sizeof(_type));                                       \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_inc_nbi(_type *fetch, _type *dest, int pe) {\
+    nbi_amo(B200SHM_AMO_FETCH_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL, \
+            fetch, sizeof(_type));                                             \
+  }                                                                            \
+  void shmem_##_tn##_atomic_compare_swap_nbi(_type *fetch, _type *dest,       \
+                                             _type cond, _type value,          \
+                                             int pe) {                         \
+    nbi_amo(B200SHM_AMO_CSWAP, B200_DTYPE_OF(_type), dest, pe, &value, &cond,  \
+            fetch, sizeof(_type));                                             \
+  }
+#define DEF_AMO_NBI_EXT(_type, _tn)                                            \
+  void shmem_##_tn##_atomic_swap_nbi(_type *fetch, _type *dest, _type value,  \
+                                     int pe) {                                 \
+    nbi_amo(B200SHM_AMO_SWAP, B200_DTYPE_OF(_type), dest, pe, &value, NULL,    \
+            fetch, sizeof(_type));                                             \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source,      \
+                                      int pe) {                                \
+    nbi_amo(B200SHM_AMO_FETCH, B200_DTYPE_OF(_type), source, pe, NULL, NULL,   \
+            fetch, sizeof(_type));                                             \
+  }
+#define DEF_AMO_NBI_BIT(_type, _tn)                                            \
+  void shmem_##_tn##_atomic_fetch_and_nbi(_type *fetch, _type *dest,          \
+                                          _type value, int pe) {               \
+    nbi_amo(B200SHM_AMO_FETCH_AND, B200_DTYPE_OF(_type), dest, pe, &value,     \
+            NULL, fetch, sizeof(_type));                                       \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_or_nbi(_type *fetch, _type *dest,           \
+                                         _type value, int pe) {                \
+    nbi_amo(B200SHM_AMO_FETCH_OR, B200_DTYPE_OF(_type), dest, pe, &value,      \
+            NULL, fetch, sizeof(_type));                                       \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_xor_nbi(_type *fetch, _type *dest,          \
+                                          _type value, int pe) {               \
+    nbi_amo(B200SHM_AMO_FETCH_XOR, B200_DTYPE_OF(_type), dest, pe, &value,     \
+            NULL, fetch, sizeof(_type));                                       \
+  }
+SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_NBI_STD)
+SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_NBI_EXT)
+SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_NBI_BIT)

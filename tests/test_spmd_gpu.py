@@ -132,3 +132,41 @@ def test_spmd_collect_matches_oracle(tmp_path, rs):
     for i in range(NC):
         x[i, :cm[i]] = (i * 16 + np.arange(cm[i])) & 0xFF
     assert o["cm"].tobytes() == rs.collect(x, cm, sum(cm)).tobytes()
+
+
+NN, NB, NADD = 8, 64, 16
+OUTN = np.dtype([("dst", np.int64, (NN, NN * NB)), ("got", np.int64, (NN, NB)),
+                 ("fetched", np.int64, (NN, NADD)), ("loc", np.uint8, (NN, NN * 32)),
+                 ("counter", np.int64), ("status", np.int32, (NN,))], align=True)
+
+
+@pytest.mark.gpu
+def test_spmd_nbi_through_the_serving_loop(tmp_path):
+    """shmem_int64_put_nbi / get_nbi, shmem_int64_atomic_fetch_add_nbi and
+    shmem_quiet: puts land in the next PE, gets bring the previous PE's
+    block, the counter adds up and hands out every value exactly once."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_nbi")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_nbi.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([exe, str(outp)], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    o = np.fromfile(outp, dtype=OUTN)[0]
+    assert (o["status"] == 0).all()
+    src = np.array([[p * 1000 + i for i in range(NB)] for p in range(NN)], np.int64)
+    for p in range(NN):
+        want = np.zeros(NN * NB, np.int64)
+        q = (p - 1) % NN
+        want[q * NB:(q + 1) * NB] = src[q]
+        assert (o["dst"][p] == want).all()
+        assert (o["got"][p] == src[(p - 1) % NN]).all()
+    assert o["counter"] == NN * NADD
+    assert sorted(o["fetched"].ravel().tolist()) == list(range(NN * NADD))
+    want_loc = np.zeros(NN * 32, np.uint8)
+    for p in range(NN):
+        want_loc[p * 32:(p + 1) * 32] = (p * 32 + np.arange(32)) & 0xFF
+    assert (o["loc"][0] == want_loc).all()
