@@ -276,8 +276,9 @@ typedef struct b200shm_server b200shm_server;
  * flight together may run in any order and concurrently, as non-blocking
  * (_nbi) operations do: a request that depends on another's result must
  * be enqueued after that one completed.  While a server runs, calls that
- * synchronise the whole device (cudaDeviceSynchronize, cudaFree) wait for
- * it to go idle. */
+ * synchronise the whole device (cudaDeviceSynchronize, cudaFree, and so
+ * b200shm_finalize) wait for it to go idle; the library's other entry
+ * points use stream-ordered memory and do not. */
 int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
                         b200shm_server **out);
 /* Validate and publish one request; *ticket identifies it.  Returns

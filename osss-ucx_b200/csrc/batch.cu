@@ -433,18 +433,22 @@ struct Batch {
    * caller's stream with events; inside a capture they become branches) */
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev; /* ev[0] = fork, ev[1 + k] = join of side[k] */
+  cudaEvent_t done = nullptr;  /* recorded after each run on the caller's stream */
 };
 
 constexpr int kBatchSideStreams = 4;
 
+/* Free a plan whose runs have completed (ordered on the library stream). */
 void release(Batch &b) {
   for (cudaStream_t x : b.side) cudaStreamDestroy(x);
   for (cudaEvent_t e : b.ev) cudaEventDestroy(e);
+  if (b.done) cudaEventDestroy(b.done);
+  b.done = nullptr;
   b.side.clear();
   b.ev.clear();
-  cudaFree(b.dd);
-  cudaFree(b.dp);
-  cudaFree(b.dcount);
+  if (b.dd) cudaFreeAsync(b.dd, st().stream);
+  if (b.dp) cudaFreeAsync(b.dp, st().stream);
+  if (b.dcount) cudaFreeAsync(b.dcount, st().stream);
   b.dd = nullptr;
   b.dp = nullptr;
   b.dcount = nullptr;
@@ -585,11 +589,16 @@ int upload(Batch &b) {
     b.groups.push_back(g);
     i = j;
   }
-  B200_CK(cudaMalloc((void **)&b.dd, nd * sizeof(BDesc)));
-  B200_CK(cudaMalloc((void **)&b.dp, (nd + 1) * sizeof(uint32_t)));
-  B200_CK(cudaMalloc((void **)&b.dcount, b.groups.size() * sizeof(unsigned)));
-  B200_CK(cudaMemcpy(b.dd, b.hd.data(), nd * sizeof(BDesc), cudaMemcpyHostToDevice));
-  B200_CK(cudaMemcpy(b.dp, b.hp.data(), (nd + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  /* stream-ordered allocations: no device-wide synchronisation, so a
+   * running serving loop does not hold them up */
+  cudaStream_t ls = st().stream;
+  B200_CK(cudaMallocAsync((void **)&b.dd, nd * sizeof(BDesc), ls));
+  B200_CK(cudaMallocAsync((void **)&b.dp, (nd + 1) * sizeof(uint32_t), ls));
+  B200_CK(cudaMallocAsync((void **)&b.dcount, b.groups.size() * sizeof(unsigned), ls));
+  B200_CK(cudaMemcpyAsync(b.dd, b.hd.data(), nd * sizeof(BDesc), cudaMemcpyHostToDevice, ls));
+  B200_CK(cudaMemcpyAsync(b.dp, b.hp.data(), (nd + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                          ls));
+  B200_CK(cudaStreamSynchronize(ls)); /* the plan is then usable on any stream */
   return B200SHM_OK;
 }
 
@@ -827,6 +836,8 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
   int rc = check_independent(descs, n);
   if (!rc) rc = upload(b);
   if (!rc) rc = make_side(b);
+  if (!rc && cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming) != cudaSuccess)
+    rc = fail(B200SHM_ERR_CUDA, "batch_create: event");
   if (rc) return bail(rc);
   if (flags & B200SHM_BATCH_GRAPH) {
     cudaStream_t cs;
@@ -862,12 +873,13 @@ int b200shm_batch_run(b200shm_batch *bh, void *stream) {
     int rc = enqueue(bh->b, s);
     if (rc) return rc;
   }
+  B200_CK(cudaEventRecord(bh->b.done, s));
   return finish(stream, "b200shm_batch_run");
 }
 
 int b200shm_batch_destroy(b200shm_batch *bh) {
   if (!bh) return B200SHM_OK;
-  cudaDeviceSynchronize();
+  if (bh->b.done) cudaEventSynchronize(bh->b.done); /* the last run, wherever it ran */
   if (bh->b.exec) cudaGraphExecDestroy(bh->b.exec);
   if (bh->b.graph) cudaGraphDestroy(bh->b.graph);
   release(bh->b);

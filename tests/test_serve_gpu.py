@@ -204,3 +204,26 @@ def test_idle_exit_and_relaunch(B, heap):
     finally:
         srv.stop()
     assert B.get_rows(a, 8, np.int64, team=(0, 1, 1))[0, 0] == 14
+
+
+def test_other_calls_do_not_wait_for_a_running_loop(B, heap):
+    """Batched reductions (stream-ordered plan memory, event-synchronised
+    destroy) and collect (stream-ordered size upload) complete while the
+    serving loop's kernel keeps running: nothing waits for the device."""
+    x = np.arange(4 * 1024, dtype=np.int32).reshape(4, 1024)
+    s, d, d2 = heap(x[0].nbytes), heap(x[0].nbytes), heap(4 * x[0].nbytes)
+    B.put_rows(s, x, team=(0, 1, 4))
+    srv = B.Server(queue_slots=4, idle_seconds=5.0)
+    try:
+        t0 = time.perf_counter()
+        items = [dict(op="sum", dtype="int32", algo="rec_dbl", team=(0, 1, 4), dest=d, src=s,
+                      nelems=1024)]
+        b = B.Batch(B.make_descs(items), B.BATCH_NO_TUNE | B.BATCH_GRAPH)
+        b.run()
+        b.close()
+        B.collect(d2, s, [4096] * 4, team=(0, 1, 4))
+        assert time.perf_counter() - t0 < 2.0
+    finally:
+        srv.stop()
+    assert (B.get_rows(d, x[0].nbytes, np.int32, team=(0, 1, 4)) == x.sum(axis=0)).all()
+    assert B.get_rows(d2, 4 * x[0].nbytes, np.uint8, team=(0, 1, 4))[1].tobytes() == x.tobytes()
