@@ -236,8 +236,8 @@ def main():
     ap.add_argument("--batch-npes", type=int, default=2048)
     ap.add_argument("--batch-teams", type=int, default=512)
     ap.add_argument("--batch-reductions", type=int, default=4096)
-    ap.add_argument("--batch-tune", default="auto", choices=["auto", "off"],
-                    help="batch workload: autotune lanes/tile per shape class, or heuristic plan")
+    ap.add_argument("--batch-tune", default="off", choices=["auto", "off"],
+                    help="batch workload: heuristic plan (off, the default) or the autotuner")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -577,7 +577,7 @@ def run_batch(args, world, rank, local):
     B.quiet()
     want = snap()
     pc_ms = timed(per_call, max(1, min(args.steps, 5)))
-    flags = B.BATCH_GRAPH | (B.BATCH_NO_TUNE if args.batch_tune == "off" else 0)
+    flags = B.BATCH_GRAPH | (B.BATCH_TUNE if args.batch_tune == "auto" else 0)
     t0 = time.perf_counter()
     descs = B.make_descs(items)
     batch = B.Batch(descs, flags)

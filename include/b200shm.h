@@ -209,13 +209,15 @@ typedef struct b200shm_reduce_desc {
 
 typedef struct b200shm_batch b200shm_batch;
 
-#define B200SHM_BATCH_NO_TUNE 0x1 /* heuristic plan, no timing runs        */
+#define B200SHM_BATCH_NO_TUNE 0x1 /* the heuristic plan (the default)      */
 #define B200SHM_BATCH_GRAPH 0x2   /* capture the run into a CUDA graph     */
+#define B200SHM_BATCH_TUNE 0x4    /* time candidate plans per shape class  */
 
 /* Plan a batch of n independent reductions: validate every descriptor,
- * let the autotuner choose lanes and tile per shape class (timing
- * candidates on the device the first time a class is seen; the choice is
- * cached for the process), and upload the plan.  The reductions run
+ * choose lanes per column, columns per lane and tile size per shape (by the
+ * measured heuristic, or with B200SHM_BATCH_TUNE by timing candidates on
+ * the device the first time a shape class is seen, cached for the process;
+ * the heuristic measured faster on mixed batches), and upload the plan.  The reductions run
  * concurrently, so a descriptor whose dest touches another descriptor's
  * source or dest (in any member) is rejected with B200SHM_ERR_ARG; sharing
  * a source, and a descriptor in place, are fine.  Replaces n separate
@@ -268,7 +270,7 @@ typedef struct b200shm_server b200shm_server;
  * mapped host memory.  Requests are cut into tiles that idle CTAs claim,
  * so a large request spreads over the GPU while small ones pass it; each
  * request reports completion through a word in host memory.  A CTA with no
- * published work for idle_seconds (0 = 1 s) exits; the host relaunches the
+ * published work for idle_seconds (0 = 0.25 s) exits; the host relaunches the
  * kernel when new work arrives, so the loop holds the GPU only while it is
  * used.  Replaces the reference's issue-one-call-and-wait model
  * (shmem_* -> shcoll / shmemc_ctx_* round trips, src/shcoll/src/*.c,
@@ -278,7 +280,11 @@ typedef struct b200shm_server b200shm_server;
  * be enqueued after that one completed.  While a server runs, calls that
  * synchronise the whole device (cudaDeviceSynchronize, cudaFree, and so
  * b200shm_finalize) wait for it to go idle; the library's other entry
- * points use stream-ordered memory and do not. */
+ * points use stream-ordered memory and do not.  The first launch of a
+ * kernel that CUDA has not loaded yet (lazy module loading, the default)
+ * also waits for the loop to go idle (at most idle_seconds; 0 = 0.25 s):
+ * run CUDA_MODULE_LOADING=EAGER, or use the calls once before starting the
+ * loop, where that matters. */
 int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
                         b200shm_server **out);
 /* Validate and publish one request; *ticket identifies it.  Returns

@@ -250,6 +250,7 @@ def amo_batch(amo, dtype, nops, pe_dev, off_dev, value_dev=None, cond_dev=None,
 # ---------------------------------------------------------------------------
 BATCH_NO_TUNE = 0x1
 BATCH_GRAPH = 0x2
+BATCH_TUNE = 0x4
 
 
 class ReduceDesc(ctypes.Structure):
@@ -341,7 +342,7 @@ def make_requests(items):
 class Server:
     """The serving loop (b200shm_serve_start / enqueue / poll / wait / stop)."""
 
-    def __init__(self, queue_slots=1024, ctas=0, idle_seconds=1.0):
+    def __init__(self, queue_slots=1024, ctas=0, idle_seconds=0.25):
         h = ctypes.c_void_p()
         _check(lib.b200shm_serve_start(queue_slots, ctas, idle_seconds, ctypes.byref(h)))
         self.h = h

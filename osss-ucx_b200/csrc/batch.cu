@@ -16,9 +16,10 @@
  * a lane combines its members in the same order as the per-call kernels
  * (a chain for order-free ops, the reference's tree shape for float
  * SUM/PROD, deferral plus exact replay for order-dependent float MIN/MAX
- * elements).  The autotuner chooses, per shape class, the lanes per
- * 16-byte column G in {1,2,4,8} and the tile size, timing the candidates
- * on the device the first time a class is seen.
+ * elements).  Per descriptor the plan picks the lanes per 16-byte column
+ * G, the columns per lane U (small teams serve 2 or 4 columns at once so a
+ * lane keeps ~8 loads in flight) and the tile size; an optional autotuner
+ * times candidate (G, tile) plans per shape class instead.
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -39,8 +40,12 @@ namespace {
 
 /* type slots of the batch kernels */
 enum { DS_I32 = 0, DS_U32, DS_I64, DS_U64, DS_F32, DS_F64, DS_N };
-/* group id: type slot, op, combine order */
-constexpr int kid_of(int ds, int op, int order) { return (ds * 7 + op) * 3 + order; }
+/* group id: type slot, op, combine order, and the column class (0, 1, 2:
+ * each lane serves 1, 2 or 4 columns at once) */
+constexpr int kbase(int ds, int op, int order) { return (ds * 7 + op) * 3 + order; }
+constexpr int kid_of(int ds, int op, int order, int uc = 0) {
+  return kbase(ds, op, order) * 3 + uc;
+}
 constexpr int kBatchThreads = 256;
 constexpr int kBatchStackLevels = 9;     /* subtree levels a lane keeps */
 constexpr int kBatchMaxLaneLeaves = 256; /* leaves per lane: 2^(levels - 1) */
@@ -53,6 +58,8 @@ struct BDesc {
   uint64_t npacks;  /* 16-byte packs of the vector part (0 if !vec)  */
   int P, p2s, logp2s, algo;
   int kid, vec, G, TP; /* TP: packs (vec) or elements (!vec) per tile */
+  int U;               /* columns each lane serves at once (small teams) */
+  int pad;
 };
 
 struct BPlan {
@@ -247,7 +254,131 @@ __device__ void run_tile(const BDesc &d, uint32_t di, uint64_t u0, uint64_t cnt,
   }
 }
 
-template <class T, int OP, int ORDER, bool MM>
+/* The small-team form of a tile: each lane serves U columns at once, so a
+ * lane of a 2-member team still has 8 loads in flight.  Chains (members in
+ * batches of 8/U per column), and butterflies whose lanes hold at most 2
+ * leaves (combined in registers per column, extras loaded alongside). */
+template <class T, int OP, int ORDER, bool MM, int V, int U>
+__device__ void run_tile_multi(const BDesc &d, uint32_t di, uint64_t u0, uint64_t cnt,
+                               const BPlan &p) {
+  typedef Pack<T, V> PK;
+  const int G = d.G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kBatchThreads >> 5;
+  const int g = lane & (G - 1), cw = lane / G, cpw = 32 / G;
+  const int P = d.P;
+  const int nleaves = ORDER == ORD_BUTTERFLY ? d.p2s : P;
+  const int l0 = (int)((long long)g * nleaves / G), l1 = (int)((long long)(g + 1) * nleaves / G);
+  auto member_of = [&](int q) -> int {
+    return ORDER == ORD_BUTTERFLY ? (int)(((long long)q * P + d.p2s - 1) >> d.logp2s) : q;
+  };
+  const int m0 = member_of(l0), m1 = member_of(l1);
+  auto comb = [](const PK &lo, const PK &hi) { return papply<OP>(lo, hi); };
+  for (uint64_t base = (uint64_t)warp * cpw * U; base < cnt; base += (uint64_t)nw * cpw * U) {
+    PK r[U];
+    unsigned cls[U][V];
+    bool live[U];
+    const char *src[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const uint64_t col = base + cw + (uint64_t)k * cpw;
+      live[k] = col < cnt;
+      src[k] = d.src + (u0 + (live[k] ? col : 0)) * V * sizeof(T);
+#pragma unroll
+      for (int i = 0; i < V; i++) cls[k][i] = 0;
+    }
+    if constexpr (ORDER == ORD_CHAIN) {
+      constexpr int MB = 8 / U; /* members per batch, per column */
+#pragma unroll
+      for (int k = 0; k < U; k++)
+        if (live[k]) {
+          r[k] = ld_pack<T, V>(src[k] + (uint64_t)m0 * d.step);
+          if constexpr (MM) {
+#pragma unroll
+            for (int i = 0; i < V; i++) cls[k][i] = fclass(r[k].x[i]);
+          }
+        }
+      for (int j = m0 + 1; j < m1; j += MB) {
+        PK x[U][MB];
+#pragma unroll
+        for (int k = 0; k < U; k++)
+#pragma unroll
+          for (int u = 0; u < MB; u++)
+            if (live[k] && j + u < m1) x[k][u] = ld_pack<T, V>(src[k] + (uint64_t)(j + u) * d.step);
+#pragma unroll
+        for (int k = 0; k < U; k++)
+#pragma unroll
+          for (int u = 0; u < MB; u++)
+            if (live[k] && j + u < m1) {
+              r[k] = papply<OP>(r[k], x[k][u]);
+              if constexpr (MM) {
+#pragma unroll
+                for (int i = 0; i < V; i++) cls[k][i] |= fclass(x[k][u].x[i]);
+              }
+            }
+      }
+    } else { /* butterfly, l1 - l0 in {1, 2} leaves per lane */
+      const int n = l1 - l0;
+      PK x[U][2], e[U][2];
+      bool ex[U][2];
+#pragma unroll
+      for (int k = 0; k < U; k++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          ex[k][u] = false;
+          if (live[k] && u < n) {
+            const int own = member_of(l0 + u);
+            x[k][u] = ld_pack<T, V>(src[k] + (uint64_t)own * d.step);
+            ex[k][u] = member_of(l0 + u + 1) - own == 2;
+            if (ex[k][u]) e[k][u] = ld_pack<T, V>(src[k] + (uint64_t)(own + 1) * d.step);
+          }
+        }
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+          if (ex[k][u]) x[k][u] = papply<OP>(e[k][u], x[k][u]); /* op(extra, own) */
+        r[k] = n == 1 ? x[k][0] : comb(x[k][0], x[k][1]);
+      }
+    }
+    for (int m = 1; m < G; m <<= 1) {
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const PK o = shfl_xor_pack<T, V>(r[k], m);
+        r[k] = (g & m) ? comb(o, r[k]) : comb(r[k], o);
+        if constexpr (MM) {
+#pragma unroll
+          for (int i = 0; i < V; i++) cls[k][i] |= __shfl_xor_sync(0xffffffffu, cls[k][i], m);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      if (!live[k]) continue;
+      const uint64_t e0 = (uint64_t)(src[k] - d.src) / sizeof(T);
+      if constexpr (MM) {
+        bool amb = false;
+#pragma unroll
+        for (int i = 0; i < V; i++) amb |= ambiguous(cls[k][i]);
+        if (amb) { /* deferred: (descriptor, element) pairs, dests untouched */
+          if (g == 0) {
+            const unsigned long long slot = atomicAdd(p.fix_count, (unsigned long long)V);
+            for (int i = 0; i < V; i++) {
+              if (slot + i < p.fix_cap)
+                p.fix_list[slot + i] = ((unsigned long long)di << 40) | (e0 + i);
+              else
+                atomicOr(p.status, (int)B200SHM_STATUS_FIX_OVERFLOW);
+            }
+          }
+          continue;
+        }
+      }
+      char *dst = d.dst + e0 * sizeof(T);
+      for (int j = m0; j < m1; j++) st_pack<T, V>(dst + (uint64_t)j * d.step, r[k]);
+    }
+  }
+}
+
+template <class T, int OP, int ORDER, bool MM, int U>
 __device__ __forceinline__ void run_desc_tile(const BDesc &d, uint32_t di, uint32_t lt,
                                               const BPlan &p, uint32_t *stk) {
   constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
@@ -255,7 +386,8 @@ __device__ __forceinline__ void run_desc_tile(const BDesc &d, uint32_t di, uint3
   if (d.vec && lt < nvt) {
     const uint64_t pb = (uint64_t)lt * d.TP;
     const uint64_t c = d.npacks - pb < (uint64_t)d.TP ? d.npacks - pb : (uint64_t)d.TP;
-    run_tile<T, OP, ORDER, MM, V>(d, di, pb, c, p, stk);
+    if constexpr (U > 1) run_tile_multi<T, OP, ORDER, MM, V, U>(d, di, pb, c, p);
+    else run_tile<T, OP, ORDER, MM, V>(d, di, pb, c, p, stk);
   } else {
     uint64_t eb, ec;
     if (d.vec) { /* the < V elements after the packs */
@@ -271,7 +403,7 @@ __device__ __forceinline__ void run_desc_tile(const BDesc &d, uint32_t di, uint3
 
 /* One (type, op, order) group of a batch: descriptors [d0, d0+nd) of the
  * plan (sorted by group), tiles taken from the group's counter. */
-template <class T, int OP, int ORDER, bool MM>
+template <class T, int OP, int ORDER, bool MM, int U>
 __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_group(const BPlan p, uint32_t d0,
                                                                uint32_t nd, unsigned *counter) {
   __shared__ unsigned s_tile;
@@ -291,7 +423,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_group(const BPlan p,
       else hi = mid;
     }
     const BDesc d = p.d[lo];
-    run_desc_tile<T, OP, ORDER, MM>(d, lo, base + t - p.prefix[lo], p, s_stk);
+    run_desc_tile<T, OP, ORDER, MM, U>(d, lo, base + t - p.prefix[lo], p, s_stk);
   }
 }
 
@@ -335,10 +467,10 @@ __global__ void __launch_bounds__(256) k_batch_fix(const BPlan p) {
     const uint64_t e = ent & ((1ull << 40) - 1);
     float *vf = (float *)vals;
     float &cf = *(float *)&common;
-    switch (d.kid) {
-    case kid_of(DS_F32, B200SHM_MIN, ORD_CHAIN): batch_fix_one<float, B200SHM_MIN>(d, e, vf, cf); break;
-    case kid_of(DS_F32, B200SHM_MAX, ORD_CHAIN): batch_fix_one<float, B200SHM_MAX>(d, e, vf, cf); break;
-    case kid_of(DS_F64, B200SHM_MIN, ORD_CHAIN): batch_fix_one<double, B200SHM_MIN>(d, e, vals, common); break;
+    switch (d.kid / 3) {
+    case kbase(DS_F32, B200SHM_MIN, ORD_CHAIN): batch_fix_one<float, B200SHM_MIN>(d, e, vf, cf); break;
+    case kbase(DS_F32, B200SHM_MAX, ORD_CHAIN): batch_fix_one<float, B200SHM_MAX>(d, e, vf, cf); break;
+    case kbase(DS_F64, B200SHM_MIN, ORD_CHAIN): batch_fix_one<double, B200SHM_MIN>(d, e, vals, common); break;
     default: batch_fix_one<double, B200SHM_MAX>(d, e, vals, common); break;
     }
   }
@@ -375,15 +507,29 @@ int log2_floor(uint64_t x) {
   return l;
 }
 
-inline int ds_of(const BDesc &d) { return d.kid / 21; }
-inline int op_of(const BDesc &d) { return (d.kid / 3) % 7; }
-inline int order_of(const BDesc &d) { return d.kid % 3; }
+inline int ds_of(const BDesc &d) { return d.kid / 3 / 21; }
+inline int op_of(const BDesc &d) { return (d.kid / 3 / 3) % 7; }
+inline int order_of(const BDesc &d) { return (d.kid / 3) % 3; }
 inline int esize_of(const BDesc &d) {
   const int ds = ds_of(d);
   return (ds == DS_I32 || ds == DS_U32 || ds == DS_F32) ? 4 : 8;
 }
 inline bool is_mm_float(const BDesc &d) {
   return ds_of(d) >= DS_F32 && (op_of(d) == B200SHM_MIN || op_of(d) == B200SHM_MAX);
+}
+
+/* Columns per lane for small teams: enough that a lane keeps about 8
+ * loads in flight (chains: members per lane <= 2 -> 4 columns, <= 4 -> 2;
+ * butterflies with at most 2 leaves per lane: 2 columns). */
+void set_columns(BDesc &d) {
+  const int order = order_of(d);
+  const int mpl = (d.P + d.G - 1) / d.G;
+  d.U = 1;
+  if (d.vec) {
+    if (order == ORD_CHAIN) d.U = mpl <= 2 ? 4 : mpl <= 4 ? 2 : 1;
+    else if (order == ORD_BUTTERFLY && d.p2s / d.G <= 2) d.U = 2;
+  }
+  d.kid = d.kid / 3 * 3 + (d.U == 4 ? 2 : d.U == 2 ? 1 : 0);
 }
 
 /* lanes per column that keep the batch kernel exact and within its stack */
@@ -485,27 +631,33 @@ BPlan plan_of(const Batch &b) {
 
 /* the group kernel of a kid, and its resident CTAs per SM */
 typedef void (*GroupKernel)(const BPlan, uint32_t, uint32_t, unsigned *);
-template <class T, int OP, int ORDER, bool MM>
+template <class T, int OP, int ORDER, bool MM, int U>
 GroupKernel gk() {
-  return k_batch_group<T, OP, ORDER, MM>;
+  return k_batch_group<T, OP, ORDER, MM, U>;
 }
-#define B200_INT_KIDS(DS, S, U)                                                             \
-  case kid_of(DS, B200SHM_AND, ORD_CHAIN): return gk<U, B200SHM_AND, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_OR, ORD_CHAIN): return gk<U, B200SHM_OR, ORD_CHAIN, false>();     \
-  case kid_of(DS, B200SHM_XOR, ORD_CHAIN): return gk<U, B200SHM_XOR, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_MIN, ORD_CHAIN): return gk<S, B200SHM_MIN, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_MAX, ORD_CHAIN): return gk<S, B200SHM_MAX, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_SUM, ORD_CHAIN): return gk<U, B200SHM_SUM, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_PROD, ORD_CHAIN): return gk<U, B200SHM_PROD, ORD_CHAIN, false>();
-#define B200_FLT_KIDS(DS, F)                                                                \
-  case kid_of(DS, B200SHM_MIN, ORD_CHAIN): return gk<F, B200SHM_MIN, ORD_CHAIN, true>();    \
-  case kid_of(DS, B200SHM_MAX, ORD_CHAIN): return gk<F, B200SHM_MAX, ORD_CHAIN, true>();    \
-  case kid_of(DS, B200SHM_SUM, ORD_CHAIN): return gk<F, B200SHM_SUM, ORD_CHAIN, false>();   \
-  case kid_of(DS, B200SHM_PROD, ORD_CHAIN): return gk<F, B200SHM_PROD, ORD_CHAIN, false>(); \
-  case kid_of(DS, B200SHM_SUM, ORD_BINOMIAL): return gk<F, B200SHM_SUM, ORD_BINOMIAL, false>(); \
-  case kid_of(DS, B200SHM_PROD, ORD_BINOMIAL): return gk<F, B200SHM_PROD, ORD_BINOMIAL, false>(); \
-  case kid_of(DS, B200SHM_SUM, ORD_BUTTERFLY): return gk<F, B200SHM_SUM, ORD_BUTTERFLY, false>(); \
-  case kid_of(DS, B200SHM_PROD, ORD_BUTTERFLY): return gk<F, B200SHM_PROD, ORD_BUTTERFLY, false>();
+#define B200_CHAIN_KIDS(DS, T_, OP_, MM_)                                               \
+  case kid_of(DS, OP_, ORD_CHAIN, 0): return gk<T_, OP_, ORD_CHAIN, MM_, 1>();          \
+  case kid_of(DS, OP_, ORD_CHAIN, 1): return gk<T_, OP_, ORD_CHAIN, MM_, 2>();          \
+  case kid_of(DS, OP_, ORD_CHAIN, 2): return gk<T_, OP_, ORD_CHAIN, MM_, 4>();
+#define B200_INT_KIDS(DS, S_, U_)                                                       \
+  B200_CHAIN_KIDS(DS, U_, B200SHM_AND, false)                                           \
+  B200_CHAIN_KIDS(DS, U_, B200SHM_OR, false)                                            \
+  B200_CHAIN_KIDS(DS, U_, B200SHM_XOR, false)                                           \
+  B200_CHAIN_KIDS(DS, S_, B200SHM_MIN, false)                                           \
+  B200_CHAIN_KIDS(DS, S_, B200SHM_MAX, false)                                           \
+  B200_CHAIN_KIDS(DS, U_, B200SHM_SUM, false)                                           \
+  B200_CHAIN_KIDS(DS, U_, B200SHM_PROD, false)
+#define B200_TREE_KIDS(DS, F_, OP_)                                                     \
+  case kid_of(DS, OP_, ORD_BINOMIAL, 0): return gk<F_, OP_, ORD_BINOMIAL, false, 1>();  \
+  case kid_of(DS, OP_, ORD_BUTTERFLY, 0): return gk<F_, OP_, ORD_BUTTERFLY, false, 1>();\
+  case kid_of(DS, OP_, ORD_BUTTERFLY, 1): return gk<F_, OP_, ORD_BUTTERFLY, false, 2>();
+#define B200_FLT_KIDS(DS, F_)                                                           \
+  B200_CHAIN_KIDS(DS, F_, B200SHM_MIN, true)                                            \
+  B200_CHAIN_KIDS(DS, F_, B200SHM_MAX, true)                                            \
+  B200_CHAIN_KIDS(DS, F_, B200SHM_SUM, false)                                           \
+  B200_CHAIN_KIDS(DS, F_, B200SHM_PROD, false)                                          \
+  B200_TREE_KIDS(DS, F_, B200SHM_SUM)                                                   \
+  B200_TREE_KIDS(DS, F_, B200SHM_PROD)
 GroupKernel group_kernel(int kid) {
   switch (kid) {
     B200_INT_KIDS(DS_I32, int32_t, uint32_t)
@@ -608,6 +760,7 @@ float time_plan(const BDesc &d0, int G, int TP, cudaStream_t s) {
   BDesc d = d0;
   d.G = G;
   d.TP = TP;
+  set_columns(d);
   t.hd.push_back(d);
   t.any_mm = is_mm_float(d);
   float best = 1e30f;
@@ -648,7 +801,10 @@ void choose_plan(BDesc &d, bool tune, cudaStream_t s) {
   }
   /* heuristic default: 2 lanes for chains, 4 for trees (the per-call
    * kernels' measured best), tiles of 1024 packs */
-  int G = order == ORD_CHAIN ? 2 : 4;
+  /* small teams: columns per lane rather than lanes per column (a
+   * butterfly over <= 8 members: lanes of 2 leaves each) */
+  int G = order == ORD_CHAIN ? (d.P <= 8 ? 1 : 2)
+                             : (order == ORD_BUTTERFLY && d.P <= 8 ? (d.p2s > 2 ? d.p2s / 2 : 1) : 4);
   while (G > 1 && !lanes_ok(d, G)) G >>= 1;
   while (!lanes_ok(d, G) && G < 8) G <<= 1;
   d.G = G;
@@ -765,7 +921,7 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
     delete bh;
     return rc;
   };
-  const bool tune = !(flags & B200SHM_BATCH_NO_TUNE);
+  const bool tune = (flags & B200SHM_BATCH_TUNE) && !(flags & B200SHM_BATCH_NO_TUNE);
   for (uint64_t i = 0; i < n; i++) {
     b200shm_reduce_desc &x = descs[i];
     if (x.algo == B200SHM_ALGO_AUTO) x.algo = B200SHM_REC_DBL;
@@ -823,11 +979,14 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
     d.npacks = d.vec ? x.nelems / (16 / es) : 0;
     d.G = 1;
     d.TP = 1024;
+    d.U = 1;
+    d.pad = 0;
     if (!lanes_ok(d, 1) && !lanes_ok(d, 2) && !lanes_ok(d, 4) && !lanes_ok(d, 8)) {
       b.fallback.push_back(x); /* trees deeper than one lane's stack */
       continue;
     }
     choose_plan(d, tune, st().stream);
+    set_columns(d);
     x.lanes = d.G;
     x.tile = d.TP;
     if (!is_int && mm) b.any_mm = true;

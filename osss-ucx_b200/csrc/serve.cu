@@ -796,7 +796,7 @@ int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
     occ = 1;
   const int cap = occ * st().sm_count;
   s->ctas = ctas > 0 ? std::min(ctas, cap) : std::min(2 * st().sm_count, cap);
-  const double idle = idle_seconds > 0 ? idle_seconds : 1.0;
+  const double idle = idle_seconds > 0 ? idle_seconds : 0.25;
   auto bail = [&](int rc) {
     if (s->h_ring) cudaFreeHost(s->h_ring);
     if (s->h_done) cudaFreeHost(s->h_done);

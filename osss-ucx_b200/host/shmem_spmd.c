@@ -466,7 +466,7 @@ static __thread int t_nbi_n, t_nbi_cap;
 
 static b200shm_server *job_server(void) {
   pthread_mutex_lock(&g_srv_mu);
-  if (!g_srv && b200shm_serve_start(4096, 0, 1.0, &g_srv) != 0) g_srv = NULL;
+  if (!g_srv && b200shm_serve_start(4096, 0, 0.25, &g_srv) != 0) g_srv = NULL;
   b200shm_server *s = g_srv;
   pthread_mutex_unlock(&g_srv_mu);
   return s;

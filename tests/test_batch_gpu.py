@@ -75,7 +75,7 @@ def check_oracle(rs, items, inputs, got, every=7):
         assert nan_equal_bytes(got[k], rs.reduce(algo, it["op"], x)), (k, it)
 
 
-@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("flags", [0, 1, 2, 3, 4, 6])
 def test_batch_matches_per_call_and_oracle(B, heap, rs, flags):
     rng = np.random.default_rng(42 + flags)
     items, inputs = make_batch(B, heap, rng, 160, B.n_pes())

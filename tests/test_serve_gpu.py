@@ -213,15 +213,20 @@ def test_other_calls_do_not_wait_for_a_running_loop(B, heap):
     x = np.arange(4 * 1024, dtype=np.int32).reshape(4, 1024)
     s, d, d2 = heap(x[0].nbytes), heap(x[0].nbytes), heap(4 * x[0].nbytes)
     B.put_rows(s, x, team=(0, 1, 4))
-    srv = B.Server(queue_slots=4, idle_seconds=5.0)
-    try:
-        t0 = time.perf_counter()
-        items = [dict(op="sum", dtype="int32", algo="rec_dbl", team=(0, 1, 4), dest=d, src=s,
-                      nelems=1024)]
-        b = B.Batch(B.make_descs(items), B.BATCH_NO_TUNE | B.BATCH_GRAPH)
+    items = [dict(op="sum", dtype="int32", algo="rec_dbl", team=(0, 1, 4), dest=d, src=s,
+                  nelems=1024)]
+
+    def calls():
+        b = B.Batch(B.make_descs(items), B.BATCH_GRAPH)
         b.run()
         b.close()
         B.collect(d2, s, [4096] * 4, team=(0, 1, 4))
+
+    calls()  # load the kernels first (CUDA loads a kernel at its first launch)
+    srv = B.Server(queue_slots=4, idle_seconds=5.0)
+    try:
+        t0 = time.perf_counter()
+        calls()
         assert time.perf_counter() - t0 < 2.0
     finally:
         srv.stop()
