@@ -55,6 +55,13 @@ extern shmem_team_t SHMEM_TEAM_WORLD;
 extern shmem_team_t SHMEM_TEAM_SHARED;
 extern shmem_team_t SHMEM_TEAM_INVALID;
 extern shmem_ctx_t SHMEM_CTX_DEFAULT;
+extern shmem_ctx_t SHMEM_CTX_INVALID;
+
+/* context options (api.h: SHMEM_CTX_SERIALIZED / PRIVATE / NOSTORE); they
+ * are accepted and recorded: every context here is thread-safe */
+#define SHMEM_CTX_SERIALIZED (1L << 0)
+#define SHMEM_CTX_PRIVATE (1L << 1)
+#define SHMEM_CTX_NOSTORE (1L << 2)
 
 /* ---- setup / query ----------------------------------------------------- */
 void shmem_init(void);
@@ -79,6 +86,23 @@ void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe);
 void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe);
 void shmem_fence(void);
 void shmem_quiet(void);
+
+/* ---- communication contexts (api.h:3619-3673, 1179-1202) ----------------
+ * A context keeps its own non-blocking operations: shmem_ctx_quiet(ctx)
+ * completes those of ctx and not those of other contexts.  A team's
+ * context takes PE numbers relative to that team. */
+int shmem_ctx_create(long options, shmem_ctx_t *ctx);
+int shmem_team_create_ctx(shmem_team_t team, long options, shmem_ctx_t *ctx);
+void shmem_ctx_destroy(shmem_ctx_t ctx);
+int shmem_ctx_get_team(shmem_ctx_t ctx, shmem_team_t *team);
+void shmem_ctx_quiet(shmem_ctx_t ctx);
+void shmem_ctx_fence(shmem_ctx_t ctx);
+void shmem_ctx_putmem(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems, int pe);
+void shmem_ctx_getmem(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems, int pe);
+void shmem_ctx_putmem_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                          int pe);
+void shmem_ctx_getmem_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                          int pe);
 
 /* ---- synchronisation --------------------------------------------------- */
 void shmem_barrier_all(void);
@@ -207,7 +231,17 @@ SHMEM_B200_TO_ALL_ARITH_TYPES(SHMEM_B200_T_PROD)
   void shmem_##_tn##_put_nbi(_type *dest, const _type *source, size_t nelems,  \
                              int pe);                                           \
   void shmem_##_tn##_get_nbi(_type *dest, const _type *source, size_t nelems,  \
-                             int pe);
+                             int pe);                                           \
+  void shmem_ctx_##_tn##_put(shmem_ctx_t ctx, _type *dest, const _type *source, \
+                             size_t nelems, int pe);                            \
+  void shmem_ctx_##_tn##_get(shmem_ctx_t ctx, _type *dest, const _type *source, \
+                             size_t nelems, int pe);                            \
+  void shmem_ctx_##_tn##_p(shmem_ctx_t ctx, _type *dest, _type value, int pe);  \
+  _type shmem_ctx_##_tn##_g(shmem_ctx_t ctx, const _type *source, int pe);      \
+  void shmem_ctx_##_tn##_put_nbi(shmem_ctx_t ctx, _type *dest,                  \
+                                 const _type *source, size_t nelems, int pe);   \
+  void shmem_ctx_##_tn##_get_nbi(shmem_ctx_t ctx, _type *dest,                  \
+                                 const _type *source, size_t nelems, int pe);
 SHMEM_B200_RMA_TYPES(SHMEM_B200_DECL_COPY)
 int shmem_fcollectmem(shmem_team_t team, void *dest, const void *source, size_t nelems);
 /* collect: each PE passes its own nelems; dest gets the contributions
@@ -272,7 +306,19 @@ void shmem_broadcast64(void *target, const void *source, size_t nelems, int PE_r
   _type shmem_##_tn##_atomic_fetch_xor(_type *dest, _type value, int pe);      \
   void shmem_##_tn##_atomic_and(_type *dest, _type value, int pe);             \
   void shmem_##_tn##_atomic_or(_type *dest, _type value, int pe);              \
-  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe);
+  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe);             \
+  _type shmem_ctx_##_tn##_atomic_fetch_and(shmem_ctx_t ctx, _type *dest,       \
+                                           _type value, int pe);                \
+  _type shmem_ctx_##_tn##_atomic_fetch_or(shmem_ctx_t ctx, _type *dest,        \
+                                          _type value, int pe);                 \
+  _type shmem_ctx_##_tn##_atomic_fetch_xor(shmem_ctx_t ctx, _type *dest,       \
+                                           _type value, int pe);                \
+  void shmem_ctx_##_tn##_atomic_and(shmem_ctx_t ctx, _type *dest, _type value, \
+                                    int pe);                                    \
+  void shmem_ctx_##_tn##_atomic_or(shmem_ctx_t ctx, _type *dest, _type value,  \
+                                   int pe);                                     \
+  void shmem_ctx_##_tn##_atomic_xor(shmem_ctx_t ctx, _type *dest, _type value, \
+                                    int pe);
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
@@ -286,18 +332,39 @@ SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
                                           _type value, int pe);                 \
   void shmem_##_tn##_atomic_fetch_inc_nbi(_type *fetch, _type *dest, int pe);  \
   void shmem_##_tn##_atomic_compare_swap_nbi(_type *fetch, _type *dest,        \
-                                             _type cond, _type value, int pe);
+                                             _type cond, _type value, int pe);  \
+  void shmem_ctx_##_tn##_atomic_fetch_add_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,         \
+                                              int pe);                          \
+  void shmem_ctx_##_tn##_atomic_fetch_inc_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, int pe);             \
+  void shmem_ctx_##_tn##_atomic_compare_swap_nbi(shmem_ctx_t ctx,              \
+                                                 _type *fetch, _type *dest,     \
+                                                 _type cond, _type value,       \
+                                                 int pe);
 #define SHMEM_B200_DECL_AMO_NBI_EXT(_type, _tn)                                 \
   void shmem_##_tn##_atomic_swap_nbi(_type *fetch, _type *dest, _type value,   \
                                      int pe);                                   \
-  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source, int pe);
+  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source, int pe); \
+  void shmem_ctx_##_tn##_atomic_swap_nbi(shmem_ctx_t ctx, _type *fetch,        \
+                                         _type *dest, _type value, int pe);     \
+  void shmem_ctx_##_tn##_atomic_fetch_nbi(shmem_ctx_t ctx, _type *fetch,       \
+                                          const _type *source, int pe);
 #define SHMEM_B200_DECL_AMO_NBI_BIT(_type, _tn)                                 \
   void shmem_##_tn##_atomic_fetch_and_nbi(_type *fetch, _type *dest,           \
                                           _type value, int pe);                 \
   void shmem_##_tn##_atomic_fetch_or_nbi(_type *fetch, _type *dest,            \
                                          _type value, int pe);                  \
   void shmem_##_tn##_atomic_fetch_xor_nbi(_type *fetch, _type *dest,           \
-                                          _type value, int pe);
+                                          _type value, int pe);                 \
+  void shmem_ctx_##_tn##_atomic_fetch_and_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,         \
+                                              int pe);                          \
+  void shmem_ctx_##_tn##_atomic_fetch_or_nbi(shmem_ctx_t ctx, _type *fetch,    \
+                                             _type *dest, _type value, int pe); \
+  void shmem_ctx_##_tn##_atomic_fetch_xor_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,         \
+                                              int pe);
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_NBI_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_NBI_BIT)

@@ -26,6 +26,10 @@ const char *shmemx_b200_last_error(void);
  * b200shm_status (the void-returning OpenSHMEM forms cannot report it). */
 int shmemx_b200_last_status(void);
 
+/* Non-blocking operations of a context that its next shmem_ctx_quiet will
+ * complete (-1 for a context that is not valid). */
+int shmemx_b200_ctx_pending(shmem_ctx_t ctx);
+
 /* Wall-clock seconds (shmemx_wtime, include/shmemx.h of the reference). */
 double shmemx_wtime(void);
 

@@ -105,7 +105,9 @@ static b200_team_t *g_actsets;  /* arrival points of the active-set forms */
 shmem_team_t SHMEM_TEAM_WORLD = &g_world;
 shmem_team_t SHMEM_TEAM_SHARED = &g_world;
 shmem_team_t SHMEM_TEAM_INVALID = NULL;
+static char g_ctx_invalid; /* a handle no context has */
 shmem_ctx_t SHMEM_CTX_DEFAULT = NULL;
+shmem_ctx_t SHMEM_CTX_INVALID = &g_ctx_invalid;
 
 static void agg_init(agg_t *g) {
   pthread_mutex_init(&g->mu, NULL);
@@ -461,8 +463,23 @@ typedef struct {
   void *fetch;
   int size;
 } nbi_t;
-static __thread nbi_t *t_nbi;
-static __thread int t_nbi_n, t_nbi_cap;
+/* the outstanding requests of one context */
+typedef struct {
+  nbi_t *v;
+  int n, cap;
+} nbi_list_t;
+/* a context made by shmem_ctx_create: its own outstanding requests on the
+ * job's one serving loop (contexts share the loop; they are completed, and
+ * quieted, independently) */
+typedef struct {
+  unsigned magic;
+  long options;
+  b200_team_t *team; /* PE numbers are relative to this team (NULL: the world) */
+  nbi_list_t list;
+} b200_ctx_t;
+#define B200_CTX_MAGIC 0xC0DE5EEDu
+static __thread nbi_list_t t_default; /* SHMEM_CTX_DEFAULT of this PE */
+#define t_nbi_n (t_default.n)
 
 static b200shm_server *job_server(void) {
   pthread_mutex_lock(&g_srv_mu);
@@ -479,21 +496,45 @@ static void stop_job_server(void) {
   pthread_mutex_unlock(&g_srv_mu);
 }
 
-/* Complete this PE's outstanding requests. */
-static int nbi_quiet(void) {
+/* Complete the outstanding requests of one context. */
+static int nbi_quiet_list(nbi_list_t *l) {
   int rc = 0;
-  for (int i = 0; i < t_nbi_n; i++) {
+  for (int i = 0; i < l->n; i++) {
     uint64_t f = 0;
-    const int r = b200shm_serve_wait(g_srv, t_nbi[i].ticket, 60.0, &f);
+    const int r = b200shm_serve_wait(g_srv, l->v[i].ticket, 60.0, &f);
     if (r) rc = engine_err(r);
-    else if (t_nbi[i].fetch) memcpy(t_nbi[i].fetch, &f, (size_t)t_nbi[i].size);
+    else if (l->v[i].fetch) memcpy(l->v[i].fetch, &f, (size_t)l->v[i].size);
   }
-  t_nbi_n = 0;
+  l->n = 0;
   return rc;
+}
+static int nbi_quiet(void) { return nbi_quiet_list(&t_default); }
+
+static b200_ctx_t *ctx_obj(shmem_ctx_t ctx) {
+  if (!ctx || ctx == SHMEM_CTX_INVALID) return NULL;
+  b200_ctx_t *c = (b200_ctx_t *)ctx;
+  return c->magic == B200_CTX_MAGIC ? c : NULL;
+}
+/* the request list of a context handle (SHMEM_CTX_DEFAULT: this PE's own) */
+static nbi_list_t *ctx_list(shmem_ctx_t ctx) {
+  if (ctx == SHMEM_CTX_DEFAULT) return &t_default;
+  b200_ctx_t *c = ctx_obj(ctx);
+  return c ? &c->list : NULL;
+}
+/* the global PE of a context's PE number (-1 when it names none, which the
+ * engine then refuses) */
+static int ctx_pe(shmem_ctx_t ctx, int pe) {
+  if (ctx == SHMEM_CTX_DEFAULT) return pe;
+  const b200_ctx_t *c = ctx_obj(ctx);
+  if (!c) return -1;
+  if (!c->team) return pe;
+  if (!c->team->valid || pe < 0 || pe >= c->team->size) return -1;
+  return c->team->start + pe * c->team->stride;
 }
 
 /* 0 when queued, 1 when the loop is unavailable (take the blocking path), <0 on error. */
-static int nbi_enqueue(const b200shm_request *r, void *fetch, int size) {
+static int nbi_enqueue_on(nbi_list_t *l, const b200shm_request *r, void *fetch, int size) {
+  if (!l) return set_err(B200SHM_ERR_ARG, "invalid context");
   b200shm_server *s = job_server();
   if (!s) return 1;
   uint64_t tk = 0;
@@ -502,32 +543,36 @@ static int nbi_enqueue(const b200shm_request *r, void *fetch, int size) {
     const int rc = b200shm_serve_enqueue(s, r, &tk);
     if (rc == 0) break;
     if (rc != B200SHM_ERR_BUSY) return engine_err(rc);
-    if (t_nbi_n) nbi_quiet(); /* free slots held by this PE */
-    else sched_yield();       /* slots held by other PEs free as the GPU completes them */
+    if (l->n) nbi_quiet_list(l); /* free slots held by this context */
+    else sched_yield();          /* other slots free as the GPU completes them */
     if (shmemx_wtime() - t0 > 60.0) return set_err(B200SHM_ERR_TIMEOUT, "nbi: no free slot");
   }
-  if (t_nbi_n == t_nbi_cap) {
-    const int cap = t_nbi_cap ? 2 * t_nbi_cap : 64;
-    nbi_t *n = (nbi_t *)realloc(t_nbi, (size_t)cap * sizeof(nbi_t));
+  if (l->n == l->cap) {
+    const int cap = l->cap ? 2 * l->cap : 64;
+    nbi_t *n = (nbi_t *)realloc(l->v, (size_t)cap * sizeof(nbi_t));
     if (!n) {
       uint64_t f = 0;
       b200shm_serve_wait(s, tk, 60.0, &f);
       if (fetch) memcpy(fetch, &f, (size_t)size);
       return 0;
     }
-    t_nbi = n;
-    t_nbi_cap = cap;
+    l->v = n;
+    l->cap = cap;
   }
-  t_nbi[t_nbi_n].ticket = tk;
-  t_nbi[t_nbi_n].fetch = fetch;
-  t_nbi[t_nbi_n].size = size;
-  t_nbi_n++;
+  l->v[l->n].ticket = tk;
+  l->v[l->n].fetch = fetch;
+  l->v[l->n].size = size;
+  l->n++;
   return 0;
+}
+static int nbi_enqueue(const b200shm_request *r, void *fetch, int size) {
+  return nbi_enqueue_on(&t_default, r, fetch, size);
 }
 
 /* put (kind PUT) or get (kind GET) of n bytes between this PE and `pe`; 1 if
  * an address is not symmetric */
-static int nbi_rma(int kind, void *dest, const void *source, size_t n, int pe) {
+static int nbi_rma(nbi_list_t *l, int kind, void *dest, const void *source, size_t n, int pe) {
+  if (!l) return set_err(B200SHM_ERR_ARG, "invalid context");
   uint64_t doff, soff;
   const char *mine = g_base + (uint64_t)t_pe * g_slice;
   const char *d = (const char *)dest, *sp = (const char *)source;
@@ -544,11 +589,11 @@ static int nbi_rma(int kind, void *dest, const void *source, size_t n, int pe) {
   r.dest_off = doff;
   r.src_off = soff;
   r.n = n;
-  return nbi_enqueue(&r, NULL, 0);
+  return nbi_enqueue_on(l, &r, NULL, 0);
 }
 
-static void nbi_amo(int op, int dtype, const void *dest, int pe, const void *value,
-                    const void *cond, void *fetch, int size) {
+static void nbi_amo(nbi_list_t *l, int op, int dtype, const void *dest, int pe,
+                    const void *value, const void *cond, void *fetch, int size) {
   uint64_t off;
   if (sym_off(dest, &off)) {
     t_status = B200SHM_ERR_ARG;
@@ -563,7 +608,7 @@ static void nbi_amo(int op, int dtype, const void *dest, int pe, const void *val
   r.dest_off = off;
   if (value) memcpy(&r.value, value, (size_t)size);
   if (cond) memcpy(&r.cond, cond, (size_t)size);
-  const int rc = nbi_enqueue(&r, fetch, size);
+  const int rc = nbi_enqueue_on(l, &r, fetch, size);
   if (rc == 1) /* no serving loop: the blocking form */
     t_status = engine_err(b200shm_amo(op, dtype, pe, off, value, cond, fetch));
   else
@@ -578,15 +623,90 @@ void shmem_getmem(void *dest, const void *source, size_t nelems, int pe) {
   uint64_t off;
   if (sym_off(source, &off) == 0) t_status = engine_err(b200shm_memcpy(dest, b200shm_ptr(pe, off), nelems, NULL));
 }
-void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
-  const int rc = nbi_rma(B200SHM_REQ_PUT, dest, source, nelems, pe);
-  if (rc == 1) shmem_putmem(dest, source, nelems, pe);
+void shmem_ctx_putmem_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                          int pe) {
+  const int g = ctx_pe(ctx, pe);
+  const int rc = nbi_rma(ctx_list(ctx), B200SHM_REQ_PUT, dest, source, nelems, g);
+  if (rc == 1) shmem_putmem(dest, source, nelems, g);
   else t_status = rc;
 }
-void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
-  const int rc = nbi_rma(B200SHM_REQ_GET, dest, source, nelems, pe);
-  if (rc == 1) shmem_getmem(dest, source, nelems, pe);
+void shmem_ctx_getmem_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                          int pe) {
+  const int g = ctx_pe(ctx, pe);
+  const int rc = nbi_rma(ctx_list(ctx), B200SHM_REQ_GET, dest, source, nelems, g);
+  if (rc == 1) shmem_getmem(dest, source, nelems, g);
   else t_status = rc;
+}
+void shmem_putmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
+  shmem_ctx_putmem_nbi(SHMEM_CTX_DEFAULT, dest, source, nelems, pe);
+}
+void shmem_getmem_nbi(void *dest, const void *source, size_t nelems, int pe) {
+  shmem_ctx_getmem_nbi(SHMEM_CTX_DEFAULT, dest, source, nelems, pe);
+}
+void shmem_ctx_putmem(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems, int pe) {
+  shmem_putmem(dest, source, nelems, ctx_pe(ctx, pe));
+}
+void shmem_ctx_getmem(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems, int pe) {
+  shmem_getmem(dest, source, nelems, ctx_pe(ctx, pe));
+}
+
+/* ---- contexts (api.h: shmem_ctx_create / destroy / quiet / fence) ---------- */
+static int ctx_make(b200_team_t *team, long options, shmem_ctx_t *ctxp) {
+  if (!ctxp) return -1;
+  *ctxp = SHMEM_CTX_INVALID;
+  if (team && !team->valid) return -1;
+  b200_ctx_t *c = (b200_ctx_t *)calloc(1, sizeof(*c));
+  if (!c) return -1;
+  c->magic = B200_CTX_MAGIC;
+  c->options = options;
+  c->team = team == &g_world ? NULL : team;
+  *ctxp = (shmem_ctx_t)c;
+  return 0;
+}
+int shmem_ctx_create(long options, shmem_ctx_t *ctxp) { return ctx_make(NULL, options, ctxp); }
+int shmem_team_create_ctx(shmem_team_t team, long options, shmem_ctx_t *ctxp) {
+  if (!team) {
+    if (ctxp) *ctxp = SHMEM_CTX_INVALID;
+    return -1;
+  }
+  return ctx_make((b200_team_t *)team, options, ctxp);
+}
+int shmem_ctx_get_team(shmem_ctx_t ctx, shmem_team_t *team) {
+  if (!team) return -1;
+  if (ctx == SHMEM_CTX_DEFAULT) {
+    *team = SHMEM_TEAM_WORLD;
+    return 0;
+  }
+  const b200_ctx_t *c = ctx_obj(ctx);
+  if (!c) {
+    *team = SHMEM_TEAM_INVALID;
+    return -1;
+  }
+  *team = c->team ? (shmem_team_t)c->team : SHMEM_TEAM_WORLD;
+  return 0;
+}
+void shmem_ctx_quiet(shmem_ctx_t ctx) {
+  nbi_list_t *l = ctx_list(ctx);
+  if (!l) {
+    t_status = set_err(B200SHM_ERR_ARG, "invalid context");
+    return;
+  }
+  const int rc = l->n ? nbi_quiet_list(l) : 0;
+  const int r2 = b200shm_quiet();
+  t_status = rc ? rc : engine_err(r2);
+}
+void shmem_ctx_fence(shmem_ctx_t ctx) { shmem_ctx_quiet(ctx); }
+int shmemx_b200_ctx_pending(shmem_ctx_t ctx) {
+  const nbi_list_t *l = ctx_list(ctx);
+  return l ? l->n : -1;
+}
+void shmem_ctx_destroy(shmem_ctx_t ctx) {
+  b200_ctx_t *c = ctx_obj(ctx);
+  if (!c) return; /* the default and invalid contexts are not destroyed */
+  shmem_ctx_quiet(ctx); /* destroying a context completes its operations */
+  free(c->list.v);
+  c->magic = 0;
+  free(c);
 }
 /* Requests in flight may complete in any order, so fence (ordering of this
  * PE's puts to one PE) is as strong as quiet here. */
@@ -598,30 +718,58 @@ void shmem_quiet(void) {
 }
 
 #define DEF_RMA(_type, _tn)                                                    \
-  void shmem_##_tn##_put(_type *dest, const _type *source, size_t nelems,     \
+  void shmem_##_tn##_put(_type *dest, const _type *source, size_t nelems,      \
                          int pe) {                                             \
     shmem_putmem(dest, source, nelems * sizeof(_type), pe);                    \
   }                                                                            \
-  void shmem_##_tn##_get(_type *dest, const _type *source, size_t nelems,     \
+  void shmem_##_tn##_get(_type *dest, const _type *source, size_t nelems,      \
                          int pe) {                                             \
     shmem_getmem(dest, source, nelems * sizeof(_type), pe);                    \
   }                                                                            \
-  void shmem_##_tn##_p(_type *dest, _type value, int pe) {                    \
+  void shmem_##_tn##_p(_type *dest, _type value, int pe) {                     \
     shmem_putmem(dest, &value, sizeof(_type), pe);                             \
   }                                                                            \
-  _type shmem_##_tn##_g(const _type *source, int pe) {                        \
+  _type shmem_##_tn##_g(const _type *source, int pe) {                         \
     _type v;                                                                   \
     memset(&v, 0, sizeof(v));                                                  \
     shmem_getmem(&v, source, sizeof(_type), pe);                               \
     return v;                                                                  \
   }                                                                            \
-  void shmem_##_tn##_put_nbi(_type *dest, const _type *source, size_t nelems, \
+  void shmem_##_tn##_put_nbi(_type *dest, const _type *source, size_t nelems,  \
                              int pe) {                                         \
     shmem_putmem_nbi(dest, source, nelems * sizeof(_type), pe);                \
   }                                                                            \
-  void shmem_##_tn##_get_nbi(_type *dest, const _type *source, size_t nelems, \
+  void shmem_##_tn##_get_nbi(_type *dest, const _type *source, size_t nelems,  \
                              int pe) {                                         \
     shmem_getmem_nbi(dest, source, nelems * sizeof(_type), pe);                \
+  }                                                                            \
+  void shmem_ctx_##_tn##_put(shmem_ctx_t ctx, _type *dest,                     \
+                             const _type *source,                              \
+                             size_t nelems, int pe) {                          \
+    shmem_ctx_putmem(ctx, dest, source, nelems * sizeof(_type), pe);           \
+  }                                                                            \
+  void shmem_ctx_##_tn##_get(shmem_ctx_t ctx, _type *dest,                     \
+                             const _type *source,                              \
+                             size_t nelems, int pe) {                          \
+    shmem_ctx_getmem(ctx, dest, source, nelems * sizeof(_type), pe);           \
+  }                                                                            \
+  void shmem_ctx_##_tn##_p(shmem_ctx_t ctx, _type *dest, _type value,          \
+                           int pe) {                                           \
+    shmem_ctx_putmem(ctx, dest, &value, sizeof(_type), pe);                    \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_g(shmem_ctx_t ctx, const _type *source, int pe) {    \
+    _type v;                                                                   \
+    memset(&v, 0, sizeof(v));                                                  \
+    shmem_ctx_getmem(ctx, &v, source, sizeof(_type), pe);                      \
+    return v;                                                                  \
+  }                                                                            \
+  void shmem_ctx_##_tn##_put_nbi(shmem_ctx_t ctx, _type *dest,                 \
+                                 const _type *source, size_t nelems, int pe) { \
+    shmem_ctx_putmem_nbi(ctx, dest, source, nelems * sizeof(_type), pe);       \
+  }                                                                            \
+  void shmem_ctx_##_tn##_get_nbi(shmem_ctx_t ctx, _type *dest,                 \
+                                 const _type *source, size_t nelems, int pe) { \
+    shmem_ctx_getmem_nbi(ctx, dest, source, nelems * sizeof(_type), pe);       \
   }
 SHMEM_B200_RMA_TYPES(DEF_RMA)
 
@@ -733,13 +881,13 @@ static int reduce_on(b200_team_t *t, int op, int dtype, int form, void *dest, co
 }
 
 #define DEF_TEAM_REDUCE(_type, _tn, _op, _OP)                                  \
-  int shmem_##_tn##_##_op##_reduce(shmem_team_t team, _type *dest,            \
-                                   const _type *source, size_t nreduce) {     \
-    return reduce_on((b200_team_t *)team, _OP, B200_DTYPE_OF(_type), 0, dest, \
+  int shmem_##_tn##_##_op##_reduce(shmem_team_t team, _type *dest,             \
+                                   const _type *source, size_t nreduce) {      \
+    return reduce_on((b200_team_t *)team, _OP, B200_DTYPE_OF(_type), 0, dest,  \
                      source, nreduce);                                         \
   }
 #define DEF_TO_ALL(_type, _tn, _op, _OP)                                       \
-  void shmem_##_tn##_##_op##_to_all(_type *dest, const _type *source,         \
+  void shmem_##_tn##_##_op##_to_all(_type *dest, const _type *source,          \
                                     int nreduce, int PE_start,                 \
                                     int logPE_stride, int PE_size,             \
                                     _type *pWrk, long *pSync) {                \
@@ -793,29 +941,29 @@ static int copy_on(b200_team_t *t, int kind, void *dest, const void *source, uin
 }
 
 #define DEF_COPY(_type, _tn)                                                   \
-  int shmem_##_tn##_fcollect(shmem_team_t team, _type *dest,                  \
-                             const _type *source, size_t nelems) {            \
+  int shmem_##_tn##_fcollect(shmem_team_t team, _type *dest,                   \
+                             const _type *source, size_t nelems) {             \
     return copy_on((b200_team_t *)team, K_FCOLLECT, dest, source,              \
                    nelems * sizeof(_type), 0, 0, 0, 0);                        \
   }                                                                            \
-  int shmem_##_tn##_collect(shmem_team_t team, _type *dest,                   \
-                            const _type *source, size_t nelems) {             \
+  int shmem_##_tn##_collect(shmem_team_t team, _type *dest,                    \
+                            const _type *source, size_t nelems) {              \
     return copy_on((b200_team_t *)team, K_COLLECT, dest, source,               \
                    nelems * sizeof(_type), 0, 0, 0, 0);                        \
   }                                                                            \
-  int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                  \
-                             const _type *source, size_t nelems) {            \
+  int shmem_##_tn##_alltoall(shmem_team_t team, _type *dest,                   \
+                             const _type *source, size_t nelems) {             \
     return copy_on((b200_team_t *)team, K_ALLTOALL, dest, source,              \
                    nelems * sizeof(_type), 0, 0, 0, 0);                        \
   }                                                                            \
-  int shmem_##_tn##_alltoalls(shmem_team_t team, _type *dest,                 \
-                              const _type *source, ptrdiff_t dst,             \
-                              ptrdiff_t sst, size_t nelems) {                 \
+  int shmem_##_tn##_alltoalls(shmem_team_t team, _type *dest,                  \
+                              const _type *source, ptrdiff_t dst,              \
+                              ptrdiff_t sst, size_t nelems) {                  \
     return copy_on((b200_team_t *)team, K_ALLTOALLS, dest, source, nelems,     \
                    dst, sst, sizeof(_type), 0);                                \
   }                                                                            \
-  int shmem_##_tn##_broadcast(shmem_team_t team, _type *dest,                 \
-                              const _type *source, size_t nelems,             \
+  int shmem_##_tn##_broadcast(shmem_team_t team, _type *dest,                  \
+                              const _type *source, size_t nelems,              \
                               int PE_root) {                                   \
     return copy_on((b200_team_t *)team, K_BROADCAST, dest, source,             \
                    nelems * sizeof(_type), 0, 0, 0, PE_root);                  \
@@ -842,21 +990,21 @@ int shmem_broadcastmem(shmem_team_t team, void *dest, const void *source, size_t
 }
 
 #define DEF_SIZED(_bits)                                                       \
-  void shmem_fcollect##_bits(void *target, const void *source, size_t nelems, \
+  void shmem_fcollect##_bits(void *target, const void *source, size_t nelems,  \
                              int PE_start, int logPE_stride, int PE_size,      \
                              long *pSync) {                                    \
     (void)pSync;                                                               \
     copy_on(active_set(PE_start, logPE_stride, PE_size), K_FCOLLECT, target,   \
             source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
   }                                                                            \
-  void shmem_collect##_bits(void *target, const void *source, size_t nelems,  \
+  void shmem_collect##_bits(void *target, const void *source, size_t nelems,   \
                             int PE_start, int logPE_stride, int PE_size,       \
                             long *pSync) {                                     \
     (void)pSync;                                                               \
     copy_on(active_set(PE_start, logPE_stride, PE_size), K_COLLECT, target,    \
             source, nelems * (_bits / 8), 0, 0, 0, 0);                         \
   }                                                                            \
-  void shmem_alltoall##_bits(void *target, const void *source, size_t nelems, \
+  void shmem_alltoall##_bits(void *target, const void *source, size_t nelems,  \
                              int PE_start, int logPE_stride, int PE_size,      \
                              long *pSync) {                                    \
     (void)pSync;                                                               \
@@ -892,113 +1040,132 @@ static void amo(int op, int dtype, const void *dest, int pe, const void *value, 
 }
 
 #define DEF_AMO_STD(_type, _tn)                                                \
-  _type shmem_##_tn##_atomic_fetch_add(_type *dest, _type value, int pe) {    \
+  _type shmem_##_tn##_atomic_fetch_add(_type *dest, _type value, int pe) {     \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH_ADD, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  void shmem_##_tn##_atomic_add(_type *dest, _type value, int pe) {           \
+  void shmem_##_tn##_atomic_add(_type *dest, _type value, int pe) {            \
     amo(B200SHM_AMO_ADD, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
   }                                                                            \
-  _type shmem_##_tn##_atomic_fetch_inc(_type *dest, int pe) {                 \
+  _type shmem_##_tn##_atomic_fetch_inc(_type *dest, int pe) {                  \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL,     \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  void shmem_##_tn##_atomic_inc(_type *dest, int pe) {                        \
+  void shmem_##_tn##_atomic_inc(_type *dest, int pe) {                         \
     amo(B200SHM_AMO_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL, NULL);    \
   }                                                                            \
-  _type shmem_##_tn##_atomic_compare_swap(_type *dest, _type cond,            \
+  _type shmem_##_tn##_atomic_compare_swap(_type *dest, _type cond,             \
                                           _type value, int pe) {               \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_CSWAP, B200_DTYPE_OF(_type), dest, pe, &value, &cond,      \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  _type shmem_ctx_##_tn##_atomic_fetch_add(shmem_ctx_t ctx, _type *dest,      \
+  _type shmem_ctx_##_tn##_atomic_fetch_add(shmem_ctx_t ctx, _type *dest,       \
                                            _type value, int pe) {              \
-    (void)ctx;                                                                 \
-    return shmem_##_tn##_atomic_fetch_add(dest, value, pe);                    \
+    return shmem_##_tn##_atomic_fetch_add(dest, value, ctx_pe(ctx, pe));       \
   }                                                                            \
-  void shmem_ctx_##_tn##_atomic_add(shmem_ctx_t ctx, _type *dest, _type value,\
+  void shmem_ctx_##_tn##_atomic_add(shmem_ctx_t ctx, _type *dest, _type value, \
                                     int pe) {                                  \
-    (void)ctx;                                                                 \
-    shmem_##_tn##_atomic_add(dest, value, pe);                                 \
+    shmem_##_tn##_atomic_add(dest, value, ctx_pe(ctx, pe));                    \
   }                                                                            \
-  _type shmem_ctx_##_tn##_atomic_fetch_inc(shmem_ctx_t ctx, _type *dest,      \
+  _type shmem_ctx_##_tn##_atomic_fetch_inc(shmem_ctx_t ctx, _type *dest,       \
                                            int pe) {                           \
-    (void)ctx;                                                                 \
-    return shmem_##_tn##_atomic_fetch_inc(dest, pe);                           \
+    return shmem_##_tn##_atomic_fetch_inc(dest, ctx_pe(ctx, pe));              \
   }                                                                            \
-  void shmem_ctx_##_tn##_atomic_inc(shmem_ctx_t ctx, _type *dest, int pe) {   \
-    (void)ctx;                                                                 \
-    shmem_##_tn##_atomic_inc(dest, pe);                                        \
+  void shmem_ctx_##_tn##_atomic_inc(shmem_ctx_t ctx, _type *dest, int pe) {    \
+    shmem_##_tn##_atomic_inc(dest, ctx_pe(ctx, pe));                           \
   }                                                                            \
-  _type shmem_ctx_##_tn##_atomic_compare_swap(shmem_ctx_t ctx, _type *dest,   \
+  _type shmem_ctx_##_tn##_atomic_compare_swap(shmem_ctx_t ctx, _type *dest,    \
                                               _type cond, _type value,         \
                                               int pe) {                        \
-    (void)ctx;                                                                 \
-    return shmem_##_tn##_atomic_compare_swap(dest, cond, value, pe);           \
+    return shmem_##_tn##_atomic_compare_swap(dest, cond, value, ctx_pe(ctx, pe)); \
   }
 #define DEF_AMO_EXT(_type, _tn)                                                \
-  _type shmem_##_tn##_atomic_swap(_type *dest, _type value, int pe) {         \
+  _type shmem_##_tn##_atomic_swap(_type *dest, _type value, int pe) {          \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_SWAP, B200_DTYPE_OF(_type), dest, pe, &value, NULL, &old); \
     return old;                                                                \
   }                                                                            \
-  void shmem_##_tn##_atomic_set(_type *dest, _type value, int pe) {           \
+  void shmem_##_tn##_atomic_set(_type *dest, _type value, int pe) {            \
     amo(B200SHM_AMO_SET, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
   }                                                                            \
-  _type shmem_##_tn##_atomic_fetch(const _type *source, int pe) {             \
+  _type shmem_##_tn##_atomic_fetch(const _type *source, int pe) {              \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH, B200_DTYPE_OF(_type), source, pe, NULL, NULL,       \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  _type shmem_ctx_##_tn##_atomic_swap(shmem_ctx_t ctx, _type *dest,           \
+  _type shmem_ctx_##_tn##_atomic_swap(shmem_ctx_t ctx, _type *dest,            \
                                       _type value, int pe) {                   \
-    (void)ctx;                                                                 \
-    return shmem_##_tn##_atomic_swap(dest, value, pe);                         \
+    return shmem_##_tn##_atomic_swap(dest, value, ctx_pe(ctx, pe));            \
   }                                                                            \
-  void shmem_ctx_##_tn##_atomic_set(shmem_ctx_t ctx, _type *dest, _type value,\
+  void shmem_ctx_##_tn##_atomic_set(shmem_ctx_t ctx, _type *dest, _type value, \
                                     int pe) {                                  \
-    (void)ctx;                                                                 \
-    shmem_##_tn##_atomic_set(dest, value, pe);                                 \
+    shmem_##_tn##_atomic_set(dest, value, ctx_pe(ctx, pe));                    \
   }                                                                            \
-  _type shmem_ctx_##_tn##_atomic_fetch(shmem_ctx_t ctx, const _type *source,  \
+  _type shmem_ctx_##_tn##_atomic_fetch(shmem_ctx_t ctx, const _type *source,   \
                                        int pe) {                               \
-    (void)ctx;                                                                 \
-    return shmem_##_tn##_atomic_fetch(source, pe);                             \
+    return shmem_##_tn##_atomic_fetch(source, ctx_pe(ctx, pe));                \
   }
 #define DEF_AMO_BIT(_type, _tn)                                                \
-  _type shmem_##_tn##_atomic_fetch_and(_type *dest, _type value, int pe) {    \
+  _type shmem_##_tn##_atomic_fetch_and(_type *dest, _type value, int pe) {     \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH_AND, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  _type shmem_##_tn##_atomic_fetch_or(_type *dest, _type value, int pe) {     \
+  _type shmem_##_tn##_atomic_fetch_or(_type *dest, _type value, int pe) {      \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH_OR, B200_DTYPE_OF(_type), dest, pe, &value, NULL,    \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  _type shmem_##_tn##_atomic_fetch_xor(_type *dest, _type value, int pe) {    \
+  _type shmem_##_tn##_atomic_fetch_xor(_type *dest, _type value, int pe) {     \
     _type old = 0;                                                             \
     amo(B200SHM_AMO_FETCH_XOR, B200_DTYPE_OF(_type), dest, pe, &value, NULL,   \
         &old);                                                                 \
     return old;                                                                \
   }                                                                            \
-  void shmem_##_tn##_atomic_and(_type *dest, _type value, int pe) {           \
+  void shmem_##_tn##_atomic_and(_type *dest, _type value, int pe) {            \
     amo(B200SHM_AMO_AND, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
   }                                                                            \
-  void shmem_##_tn##_atomic_or(_type *dest, _type value, int pe) {            \
+  void shmem_##_tn##_atomic_or(_type *dest, _type value, int pe) {             \
     amo(B200SHM_AMO_OR, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);   \
   }                                                                            \
-  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe) {           \
+  void shmem_##_tn##_atomic_xor(_type *dest, _type value, int pe) {            \
     amo(B200SHM_AMO_XOR, B200_DTYPE_OF(_type), dest, pe, &value, NULL, NULL);  \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch_and(shmem_ctx_t ctx, _type *dest,       \
+                                           _type value,                        \
+                                          int pe) {                            \
+    return shmem_##_tn##_atomic_fetch_and(dest, value, ctx_pe(ctx, pe));       \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_and(shmem_ctx_t ctx, _type *dest,              \
+                                    _type value, int pe) {                     \
+    shmem_##_tn##_atomic_and(dest, value, ctx_pe(ctx, pe));                    \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch_or(shmem_ctx_t ctx, _type *dest,        \
+                                          _type value,                         \
+                                          int pe) {                            \
+    return shmem_##_tn##_atomic_fetch_or(dest, value, ctx_pe(ctx, pe));        \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_or(shmem_ctx_t ctx, _type *dest,               \
+                                   _type value, int pe) {                      \
+    shmem_##_tn##_atomic_or(dest, value, ctx_pe(ctx, pe));                     \
+  }                                                                            \
+  _type shmem_ctx_##_tn##_atomic_fetch_xor(shmem_ctx_t ctx, _type *dest,       \
+                                           _type value,                        \
+                                          int pe) {                            \
+    return shmem_##_tn##_atomic_fetch_xor(dest, value, ctx_pe(ctx, pe));       \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_xor(shmem_ctx_t ctx, _type *dest,              \
+                                    _type value, int pe) {                     \
+    shmem_##_tn##_atomic_xor(dest, value, ctx_pe(ctx, pe));                    \
   }
 SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_EXT)
@@ -1006,47 +1173,92 @@ SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_BIT)
 
 /* the fetching atomics' _nbi forms: the old value lands in *fetch at quiet */
 #define DEF_AMO_NBI_STD(_type, _tn)                                            \
-  void shmem_##_tn##_atomic_fetch_add_nbi(_type *fetch, _type *dest,          \
+  void shmem_ctx_##_tn##_atomic_fetch_add_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,        \
+                                              int pe) {                        \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH_ADD, B200_DTYPE_OF(_type),        \
+            dest, ctx_pe(ctx, pe), &value, NULL, fetch, sizeof(_type));        \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_add_nbi(_type *fetch, _type *dest,           \
                                           _type value, int pe) {               \
-    nbi_amo(B200SHM_AMO_FETCH_ADD, B200_DTYPE_OF(_type), dest, pe, &value,     \
-            NULL, fetch, sizeof(_type));                                       \
+    shmem_ctx_##_tn##_atomic_fetch_add_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
+                                           value, pe);                         \
   }                                                                            \
-  void shmem_##_tn##_atomic_fetch_inc_nbi(_type *fetch, _type *dest, int pe) {\
-    nbi_amo(B200SHM_AMO_FETCH_INC, B200_DTYPE_OF(_type), dest, pe, NULL, NULL, \
-            fetch, sizeof(_type));                                             \
+  void shmem_ctx_##_tn##_atomic_fetch_inc_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, int pe) {           \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH_INC, B200_DTYPE_OF(_type),        \
+            dest, ctx_pe(ctx, pe), NULL, NULL, fetch, sizeof(_type));          \
   }                                                                            \
-  void shmem_##_tn##_atomic_compare_swap_nbi(_type *fetch, _type *dest,       \
+  void shmem_##_tn##_atomic_fetch_inc_nbi(_type *fetch, _type *dest, int pe) { \
+    shmem_ctx_##_tn##_atomic_fetch_inc_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
+                                           pe);                                \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_compare_swap_nbi(shmem_ctx_t ctx,              \
+                                                 _type *fetch, _type *dest,    \
+                                                 _type cond, _type value,      \
+                                                 int pe) {                     \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_CSWAP, B200_DTYPE_OF(_type), dest,      \
+            ctx_pe(ctx, pe), &value, &cond, fetch, sizeof(_type));             \
+  }                                                                            \
+  void shmem_##_tn##_atomic_compare_swap_nbi(_type *fetch, _type *dest,        \
                                              _type cond, _type value,          \
                                              int pe) {                         \
-    nbi_amo(B200SHM_AMO_CSWAP, B200_DTYPE_OF(_type), dest, pe, &value, &cond,  \
-            fetch, sizeof(_type));                                             \
+    shmem_ctx_##_tn##_atomic_compare_swap_nbi(SHMEM_CTX_DEFAULT, fetch,        \
+                                              dest, cond, value, pe);          \
   }
 #define DEF_AMO_NBI_EXT(_type, _tn)                                            \
-  void shmem_##_tn##_atomic_swap_nbi(_type *fetch, _type *dest, _type value,  \
-                                     int pe) {                                 \
-    nbi_amo(B200SHM_AMO_SWAP, B200_DTYPE_OF(_type), dest, pe, &value, NULL,    \
-            fetch, sizeof(_type));                                             \
+  void shmem_ctx_##_tn##_atomic_swap_nbi(shmem_ctx_t ctx, _type *fetch,        \
+                                         _type *dest, _type value, int pe) {   \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_SWAP, B200_DTYPE_OF(_type), dest,       \
+            ctx_pe(ctx, pe), &value, NULL, fetch, sizeof(_type));              \
   }                                                                            \
-  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source,      \
+  void shmem_##_tn##_atomic_swap_nbi(_type *fetch, _type *dest, _type value,   \
+                                     int pe) {                                 \
+    shmem_ctx_##_tn##_atomic_swap_nbi(SHMEM_CTX_DEFAULT, fetch, dest, value,   \
+                                      pe);                                     \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_fetch_nbi(shmem_ctx_t ctx, _type *fetch,       \
+                                          const _type *source, int pe) {       \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH, B200_DTYPE_OF(_type), source,    \
+            ctx_pe(ctx, pe), NULL, NULL, fetch, sizeof(_type));                \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_nbi(_type *fetch, const _type *source,       \
                                       int pe) {                                \
-    nbi_amo(B200SHM_AMO_FETCH, B200_DTYPE_OF(_type), source, pe, NULL, NULL,   \
-            fetch, sizeof(_type));                                             \
+    shmem_ctx_##_tn##_atomic_fetch_nbi(SHMEM_CTX_DEFAULT, fetch, source, pe);  \
   }
 #define DEF_AMO_NBI_BIT(_type, _tn)                                            \
-  void shmem_##_tn##_atomic_fetch_and_nbi(_type *fetch, _type *dest,          \
-                                          _type value, int pe) {               \
-    nbi_amo(B200SHM_AMO_FETCH_AND, B200_DTYPE_OF(_type), dest, pe, &value,     \
-            NULL, fetch, sizeof(_type));                                       \
+  void shmem_ctx_##_tn##_atomic_fetch_and_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,        \
+                                              int pe) {                        \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH_AND, B200_DTYPE_OF(_type),        \
+            dest, ctx_pe(ctx, pe), &value, NULL, fetch, sizeof(_type));        \
   }                                                                            \
-  void shmem_##_tn##_atomic_fetch_or_nbi(_type *fetch, _type *dest,           \
+  void shmem_##_tn##_atomic_fetch_and_nbi(_type *fetch, _type *dest,           \
+                                          _type value, int pe) {               \
+    shmem_ctx_##_tn##_atomic_fetch_and_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
+                                           value, pe);                         \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_fetch_or_nbi(shmem_ctx_t ctx, _type *fetch,    \
+                                             _type *dest, _type value,         \
+                                             int pe) {                         \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH_OR, B200_DTYPE_OF(_type), dest,   \
+            ctx_pe(ctx, pe), &value, NULL, fetch, sizeof(_type));              \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_or_nbi(_type *fetch, _type *dest,            \
                                          _type value, int pe) {                \
-    nbi_amo(B200SHM_AMO_FETCH_OR, B200_DTYPE_OF(_type), dest, pe, &value,      \
-            NULL, fetch, sizeof(_type));                                       \
+    shmem_ctx_##_tn##_atomic_fetch_or_nbi(SHMEM_CTX_DEFAULT, fetch, dest,      \
+                                          value, pe);                          \
   }                                                                            \
-  void shmem_##_tn##_atomic_fetch_xor_nbi(_type *fetch, _type *dest,          \
+  void shmem_ctx_##_tn##_atomic_fetch_xor_nbi(shmem_ctx_t ctx, _type *fetch,   \
+                                              _type *dest, _type value,        \
+                                              int pe) {                        \
+    nbi_amo(ctx_list(ctx), B200SHM_AMO_FETCH_XOR, B200_DTYPE_OF(_type),        \
+            dest, ctx_pe(ctx, pe), &value, NULL, fetch, sizeof(_type));        \
+  }                                                                            \
+  void shmem_##_tn##_atomic_fetch_xor_nbi(_type *fetch, _type *dest,           \
                                           _type value, int pe) {               \
-    nbi_amo(B200SHM_AMO_FETCH_XOR, B200_DTYPE_OF(_type), dest, pe, &value,     \
-            NULL, fetch, sizeof(_type));                                       \
+    shmem_ctx_##_tn##_atomic_fetch_xor_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
+                                           value, pe);                         \
   }
 SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_NBI_EXT)

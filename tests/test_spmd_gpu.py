@@ -170,3 +170,57 @@ def test_spmd_nbi_through_the_serving_loop(tmp_path):
     for p in range(NN):
         want_loc[p * 32:(p + 1) * 32] = (p * 32 + np.arange(32)) & 0xFF
     assert (o["loc"][0] == want_loc).all()
+
+
+TP = 4
+OUTC = np.dtype([("dst", np.int64, (NN, NN * NB)), ("tdst", np.int64, (NN, TP * NB)),
+                 ("fa", np.int64, (NN, NADD)), ("fc", np.int64, (NN,)), ("g", np.int64, (NN,)),
+                 ("counter", np.int64), ("counter2", np.int64), ("bits", np.int64),
+                 ("pending", np.int32, (NN, 6)), ("create_rc", np.int32, (NN,)),
+                 ("team_rc", np.int32, (NN,)), ("team_ok", np.int32, (NN,)),
+                 ("invalid_status", np.int32, (NN,)), ("status", np.int32, (NN,))], align=True)
+
+
+@pytest.mark.gpu
+def test_spmd_contexts_quiet_independently(tmp_path):
+    """shmem_ctx_create / quiet / destroy, shmem_team_create_ctx: quieting one
+    context completes its operations and leaves another's pending; a team
+    context takes team-relative PE numbers; destroying a context completes
+    it; SHMEM_CTX_INVALID is refused."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_ctx")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_ctx.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([exe, str(outp)], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert os.path.getsize(outp) == OUTC.itemsize
+    o = np.fromfile(outp, dtype=OUTC)[0]
+    assert (o["status"] == 0).all() and (o["create_rc"] == 0).all()
+    assert (o["pending"] == [NADD, 1, 0, 1, 0, 0]).all(), o["pending"]
+    assert o["counter"] == NN * NADD
+    assert sorted(o["fa"].ravel().tolist()) == list(range(NN * NADD))
+    src = np.array([[p * 1000 + i for i in range(NB)] for p in range(NN)], np.int64)
+    for p in range(NN):
+        want = np.zeros(NN * NB, np.int64)
+        q = (p - 1) % NN
+        want[q * NB:(q + 1) * NB] = src[q]
+        assert (o["dst"][p] == want).all()
+    even = list(range(0, NN, 2))
+    assert [int(v == 0) for v in o["team_rc"]] == [int(p in even) for p in range(NN)]
+    assert (o["team_ok"] == 1).all()
+    for p in even:
+        want = np.zeros(TP * NB, np.int64)
+        tq = (p // 2 - 1) % TP
+        want[tq * NB:(tq + 1) * NB] = src[2 * tq]
+        assert (o["tdst"][p] == want).all()
+    for p in range(1, NN, 2):
+        assert (o["tdst"][p] == 0).all()
+    assert o["bits"] == sum(1 << p for p in even)
+    assert o["counter2"] == NN and sorted(o["fc"].tolist()) == list(range(NN))
+    assert (o["invalid_status"] < 0).all()
+    assert (o["g"] == np.arange(NN)).all()
