@@ -173,7 +173,7 @@ def test_spmd_nbi_through_the_serving_loop(tmp_path):
 
 
 TP = 4
-OUTC = np.dtype([("dst", np.int64, (NN, NN * NB)), ("tdst", np.int64, (NN, TP * NB)),
+OUTX = np.dtype([("dst", np.int64, (NN, NN * NB)), ("tdst", np.int64, (NN, TP * NB)),
                  ("fa", np.int64, (NN, NADD)), ("fc", np.int64, (NN,)), ("g", np.int64, (NN,)),
                  ("counter", np.int64), ("counter2", np.int64), ("bits", np.int64),
                  ("pending", np.int32, (NN, 6)), ("create_rc", np.int32, (NN,)),
@@ -198,8 +198,8 @@ def test_spmd_contexts_quiet_independently(tmp_path):
     r = subprocess.run([exe, str(outp)], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M"),
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    assert os.path.getsize(outp) == OUTC.itemsize
-    o = np.fromfile(outp, dtype=OUTC)[0]
+    assert os.path.getsize(outp) == OUTX.itemsize
+    o = np.fromfile(outp, dtype=OUTX)[0]
     assert (o["status"] == 0).all() and (o["create_rc"] == 0).all()
     assert (o["pending"] == [NADD, 1, 0, 1, 0, 0]).all(), o["pending"]
     assert o["counter"] == NN * NADD
