@@ -35,6 +35,7 @@
 #include <string.h>
 
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 #include <type_traits>
 
@@ -379,33 +380,74 @@ unsigned reduce_grid(K kernel, int &occ, uint64_t nvec, int threads) {
   return (unsigned)(need < cap ? (need ? need : 1) : cap);
 }
 
+/* CTAs of 256 threads of `kernel` that one SM holds at once (cached per
+ * kernel). */
+int resident_ctas(const void *kernel) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0) != cudaSuccess || n < 1) {
+    (void)cudaGetLastError();
+    n = 1;
+  }
+  cache[kernel] = n;
+  return n;
+}
+
+/* Grid of the warp-cooperative kernel, in waves of the CTAs one SM holds
+ * at once: 8 waves by default (B200SHM_REDUCE_WAVES overrides it, or
+ * B200SHM_REDUCE_CTAS_PER_SM gives a fixed count).  On the 64-PE x 2^20
+ * workload one exact wave was slowest (5.27 TB/s over the six
+ * reductions): CTAs of a grid-stride loop finish unevenly and leave their
+ * SM's slots idle, while the CTAs of later waves backfill them.  4 waves
+ * gave 5.73, 6-16 waves 5.78-5.80, one pack per lane 5.76. */
+unsigned coop_grid(const void *kernel, uint64_t lanes) {
+  static int per_sm_env = -1, waves = 8;
+  if (per_sm_env < 0) {
+    const char *e = getenv("B200SHM_REDUCE_CTAS_PER_SM");
+    per_sm_env = e && atoi(e) > 0 ? atoi(e) : 0;
+    const char *w = getenv("B200SHM_REDUCE_WAVES");
+    if (w && atoi(w) > 0) waves = atoi(w);
+  }
+  const int per_sm = per_sm_env ? per_sm_env : waves * resident_ctas(kernel);
+  return grid_for(lanes, 256, per_sm);
+}
+
+template <class K>
+void launch_one(K kernel, uint64_t lanes, cudaStream_t s, const RArgs &a) {
+  kernel<<<coop_grid((const void *)kernel, lanes), 256, 0, s>>>(a);
+}
+
 template <class T, int OP, int ORDER, int V, bool MM, int G>
-void launch_coop_g(int lvl, bool pow2, unsigned grid, cudaStream_t s, const RArgs &a) {
+void launch_coop_g(int lvl, bool pow2, uint64_t lanes, cudaStream_t s, const RArgs &a) {
   if constexpr (ORDER == ORD_CHAIN) {
-    k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
+    launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true>, lanes, s, a);
   } else if constexpr (ORDER == ORD_BINOMIAL) { /* only power-of-two teams get here */
-    if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
-    else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true><<<grid, 256, 0, s>>>(a);
-    else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true><<<grid, 256, 0, s>>>(a);
+    if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true>, lanes, s, a);
+    else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true>, lanes, s, a);
+    else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true>, lanes, s, a);
   } else {
     if (pow2) {
-      if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true><<<grid, 256, 0, s>>>(a);
-      else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true><<<grid, 256, 0, s>>>(a);
-      else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true><<<grid, 256, 0, s>>>(a);
+      if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true>, lanes, s, a);
+      else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true>, lanes, s, a);
+      else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true>, lanes, s, a);
     } else {
-      if (lvl == 1) k_reduce_coop<T, OP, ORDER, V, G, MM, 1, false><<<grid, 256, 0, s>>>(a);
-      else if (lvl == 2) k_reduce_coop<T, OP, ORDER, V, G, MM, 2, false><<<grid, 256, 0, s>>>(a);
-      else k_reduce_coop<T, OP, ORDER, V, G, MM, 7, false><<<grid, 256, 0, s>>>(a);
+      if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, false>, lanes, s, a);
+      else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, false>, lanes, s, a);
+      else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, false>, lanes, s, a);
     }
   }
 }
 
 template <class T, int OP, int ORDER, int V, bool MM>
-void launch_coop(int G, int lvl, bool pow2, unsigned grid, cudaStream_t s, const RArgs &a) {
+void launch_coop(int G, int lvl, bool pow2, uint64_t lanes, cudaStream_t s, const RArgs &a) {
   switch (G) {
-  case 2: launch_coop_g<T, OP, ORDER, V, MM, 2>(lvl, pow2, grid, s, a); break;
-  case 4: launch_coop_g<T, OP, ORDER, V, MM, 4>(lvl, pow2, grid, s, a); break;
-  default: launch_coop_g<T, OP, ORDER, V, MM, 8>(lvl, pow2, grid, s, a); break;
+  case 2: launch_coop_g<T, OP, ORDER, V, MM, 2>(lvl, pow2, lanes, s, a); break;
+  case 4: launch_coop_g<T, OP, ORDER, V, MM, 4>(lvl, pow2, lanes, s, a); break;
+  default: launch_coop_g<T, OP, ORDER, V, MM, 8>(lvl, pow2, lanes, s, a); break;
   }
 }
 
@@ -440,11 +482,10 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
       if constexpr (ORDER != ORD_CHAIN || any_order) {
         if (splittable && G >= 2) {
           const uint64_t lanes = a.nvec * (uint64_t)G;
-          const unsigned grid = grid_for(lanes, 256, 8);
           const int chunks = nleaves / G / 8; /* tree chunks per lane */
           const bool pow2 = ORDER != ORD_BUTTERFLY || base.P == base.p2s;
           launch_coop<T, OP, ORDER, V, MM>(G, ORDER == ORD_CHAIN ? 1 : chunks <= 1 ? 1 : chunks == 2 ? 2 : 7,
-                                           pow2, grid, s, a);
+                                           pow2, lanes, s, a);
           count_launch();
           done += a.nvec * V;
         }

@@ -10,12 +10,15 @@
  *
  *  - the host writes a request into its ring slot (sequence word last) and
  *    then the ring's tail, both with release ordering;
+ *  - one CTA at a time copies newly published requests into device memory
+ *    (the mirror) and opens each to claims by setting its slot's claim
+ *    word;
  *  - every request is cut into tiles on the host (a range of elements of a
- *    reduction, a chunk or a run of segments of a copy, one atomic), and a
- *    single device cursor (request << 24 | tile) hands tiles out: a CTA
- *    claims (r, t) only when request r is published, with a compare-and-
- *    swap, so no CTA ever holds a claim it cannot serve and no CTA ever
- *    waits for another CTA;
+ *    reduction, a chunk or a run of segments of a copy, one atomic) and
+ *    its tiles into at most one share per CTA; a CTA claims a share with
+ *    one fetch-and-add on the slot's claim word, only on requests already
+ *    mirrored, so no CTA ever holds a claim it cannot serve and no CTA
+ *    ever waits for another CTA;
  *  - the CTA that finishes a request's last tile writes its completion word
  *    (sequence, AMO old value, status) to host memory after a system-scope
  *    fence;
@@ -29,6 +32,7 @@
  * the algorithm's tree for float SUM/PROD, an exact replay for float
  * MIN/MAX elements whose result depends on operand order).
  */
+#include <stddef.h>
 #include <stdint.h>
 #include <string.h>
 #include <time.h>
@@ -47,8 +51,21 @@ namespace b200 {
 namespace {
 
 constexpr int kServeThreads = 256;
-constexpr int kTileBits = 24;
-constexpr unsigned long long kTileMask = (1ull << kTileBits) - 1;
+/* The claim word of a ring slot: [63:40] the request it serves (its low 24
+ * bits), [39:24] the number of shares its tiles are cut into, [23:0] the
+ * next share to hand out. */
+constexpr int kTagShift = 40, kShareShift = 24;
+constexpr unsigned long long kField24 = (1ull << 24) - 1;
+constexpr unsigned long long kTileLimit = 1ull << 22;
+__host__ __device__ __forceinline__ unsigned long long claim_word(unsigned long long r,
+                                                                  unsigned long long nshares) {
+  return ((r & kField24) << kTagShift) | (nshares << kShareShift);
+}
+/* tiles per share: at most one share per CTA */
+__host__ __device__ __forceinline__ unsigned long long share_tiles(unsigned long long ntiles,
+                                                                   unsigned ctas) {
+  return (ntiles + ctas - 1) / ctas;
+}
 constexpr uint64_t kCopyChunk = 32u << 10;       /* bytes per copy tile            */
 constexpr uint64_t kReduceTileRead = 256u << 10; /* source bytes per reduce tile   */
 
@@ -64,6 +81,8 @@ struct alignas(16) SReq {
   unsigned long long pad;
 };
 static_assert(sizeof(SReq) == 128, "ring slot of 128 bytes");
+static_assert(offsetof(SReq, ntiles) == 9 * 8 && offsetof(SReq, seq) == 14 * 8,
+              "the mirror reads ntiles as word 9 and publishes seq as word 14");
 
 /* A completion word (mapped host memory, written by the device), with the
  * device clock (globaltimer, ns) when the request was copied from the
@@ -98,7 +117,7 @@ struct SArgs {
   const SCtl *ctl;
   SDev *dev;
   unsigned int *tiles_done; /* per slot */
-  unsigned long long *tctr; /* per slot: (request << 24) | next tile, set when mirrored */
+  unsigned long long *tctr; /* per slot: the claim word, set when the request is mirrored */
   SReq *mreq;               /* per slot: device copy of the request (seq = ticket + 1) */
   unsigned int Q;
   char *base;
@@ -157,18 +176,24 @@ constexpr unsigned long long kMirrorBatch = kServeThreads / 16; /* requests one 
  * into device memory (the CTA copies them, then publishes and releases the
  * lock); or 0 when the CTA should exit (stop requested or idle past the
  * limit, in both cases holding no claim).
- * Tiles come from a per-slot counter tagged with the request it serves, by
- * fetch-and-add: every CTA gets a distinct share in one atomic.  An add that
+ * A claim is one fetch-and-add of 1 on the slot's claim word, which says
+ * by itself whether a share was left: no request descriptor is read before
+ * the claim, and a CTA that finds nothing left walks on to the next
+ * request at once (the cursor is only a hint of where unclaimed shares
+ * start; whoever takes a request's last share moves it on).  An add that
  * lands after the slot moved on to a later request x (only possible once
  * the request it aimed at is complete) holds a share of x, which is served
- * as such, so no tile is ever lost or handed out twice. */
+ * as such, so no tile is ever lost or handed out twice.  *r_hint carries
+ * the request this CTA looks at next from one claim to the next. */
 __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned long long *ct,
                      unsigned *count, unsigned long long *mfrom, unsigned long long *mupto,
-                     unsigned long long idle_since) {
+                     unsigned long long idle_since, unsigned long long *r_hint) {
   unsigned backoff = 32;
+  unsigned long long r = *r_hint;
   for (;;) {
-    const unsigned long long r = vld(&a.dev->cursor);
-    unsigned long long tl = vld(&a.dev->tail_mirror);
+    const unsigned long long cur = vld(&a.dev->cursor);
+    const unsigned long long tl = vld(&a.dev->tail_mirror);
+    if (cur > r) r = cur;
     if (r >= tl) {
       /* test, then test-and-set: waiting CTAs only read the lock word */
       if (*(const volatile unsigned *)&a.dev->poll_lock == 0u &&
@@ -179,11 +204,12 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
         if (ht > mt) { /* the whole CTA copies them, still holding the lock */
           *mfrom = mt;
           *mupto = ht < mt + kMirrorBatch ? ht : mt + kMirrorBatch;
+          *r_hint = r;
           return 2;
         }
         atomicExch(&a.dev->poll_lock, 0u);
       }
-      if (r >= tl) {
+      if (vld(&a.dev->tail_mirror) <= r) {
         /* only the lock holder reads host memory: a read of host memory by
          * every waiting CTA on every turn floods the path to the host and
          * stalls every other memory access behind it */
@@ -191,28 +217,28 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
         if (now_ns() - idle_since > a.idle_ns) return 0;
         __nanosleep(backoff);
         backoff = backoff < 512 ? backoff * 2 : 512;
-        continue;
       }
-    }
-    fence_gpu();
-    if (req->seq != r + 1 && !read_req(a, r, req)) { /* recycled: r is complete */
-      atomicCAS(&a.dev->cursor, r, r + 1);
       continue;
     }
-    const unsigned long long k = (req->ntiles + gridDim.x - 1) / gridDim.x;
-    const unsigned long long old = atomicAdd(&a.tctr[r % a.Q], k);
-    const unsigned long long x = old >> kTileBits, c = old & kTileMask;
-    if (x != r) { /* the slot serves a later request x by now */
+    fence_gpu(); /* the claim words of requests below tail_mirror are set */
+    for (; r < tl; r++) {
+      const unsigned long long old = atomicAdd(&a.tctr[r % a.Q], 1ull);
+      const unsigned long long x = r + (((old >> kTagShift) - r) & kField24);
+      const unsigned long long nsh = (old >> kShareShift) & 0xFFFFull, sh = old & kField24;
+      /* r is handed out: the cursor moves past it (a CTA that finds the
+       * shares gone leaves that to the one that took the last) */
+      if (x != r || sh + 1 == nsh) atomicMax(&a.dev->cursor, r + 1);
+      if (sh >= nsh) continue;
+      /* share sh of request x is ours; x stays in its slot until it completes */
       fence_gpu();
-      if (!read_req(a, x, req)) continue;
-    }
-    if (c < req->ntiles) {
+      if (req->seq != x + 1 && !read_req(a, x, req)) continue; /* not reached */
+      const unsigned long long k = share_tiles(req->ntiles, gridDim.x);
       *cr = x;
-      *ct = c;
-      *count = (unsigned)(req->ntiles - c < k ? req->ntiles - c : k);
+      *ct = sh * k;
+      *count = (unsigned)(req->ntiles - sh * k < k ? req->ntiles - sh * k : k);
+      *r_hint = x == r && sh + 1 < nsh ? r : r + 1;
       return 1;
     }
-    atomicCAS(&a.dev->cursor, r, r + 1); /* all of r's tiles are handed out */
   }
 }
 
@@ -526,12 +552,21 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
   }
   fence_gpu();
   __syncthreads();
+  if (threadIdx.x < n) {
+    const unsigned long long x = from + threadIdx.x;
+    ((volatile unsigned long long *)&a.mreq[x % a.Q])[14] = x + 1;
+  }
+  fence_gpu();
+  __syncthreads();
+  if (threadIdx.x < n) { /* the claim word last: it opens the request to claims */
+    const unsigned long long x = from + threadIdx.x;
+    const unsigned long long nt = ((const volatile unsigned long long *)&a.mreq[x % a.Q])[9];
+    const unsigned long long k = share_tiles(nt, gridDim.x);
+    atomicExch(&a.tctr[x % a.Q], claim_word(x, (nt + k - 1) / k));
+  }
+  fence_gpu();
+  __syncthreads();
   if (threadIdx.x == 0) {
-    for (unsigned long long x = from; x < upto; x++)
-      ((volatile unsigned long long *)&a.mreq[x % a.Q])[14] = x + 1;
-    fence_gpu();
-    for (unsigned long long x = from; x < upto; x++) atomicExch(&a.tctr[x % a.Q], x << kTileBits);
-    fence_gpu();
     *(volatile unsigned long long *)&a.dev->tail_mirror = upto;
     fence_gpu();
     atomicExch(&a.dev->poll_lock, 0u);
@@ -549,10 +584,11 @@ __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
   __shared__ int s_status;
   __shared__ unsigned long long s_tclaim;
   unsigned long long idle_since = now_ns();
+  unsigned long long r_hint = 0;
   if (threadIdx.x == 0) s_req.seq = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      s_go = claim(a, &s_req, &s_cr, &s_ct, &s_count, &s_mfrom, &s_mupto, idle_since);
+      s_go = claim(a, &s_req, &s_cr, &s_ct, &s_count, &s_mfrom, &s_mupto, idle_since, &r_hint);
       s_tclaim = now_ns();
       s_fetched = 0;
       s_status = 0;
@@ -766,9 +802,10 @@ int plan_request(const b200shm_request &r0, SReq *q) {
     }
     if (q->ntiles == 0) q->ntiles = 1;
   }
-  /* shares handed out past the last tile stay below twice the tiles plus
-   * one share per CTA, inside the counter's 24 bits */
-  if (q->ntiles > (kTileMask >> 2))
+  /* a request is cut into at most one share per CTA; the adds that land
+   * on its claim word past the last share are at most a few per CTA, far
+   * inside the word's 24-bit share field */
+  if (q->ntiles > kTileLimit)
     return fail(B200SHM_ERR_ARG, "serve: request of more than 2^22 tiles");
   return B200SHM_OK;
 }
