@@ -101,6 +101,10 @@ struct SCtl {
   unsigned long long tail; /* requests published */
   int stop;
   int pad[13];
+  /* written by the device: the launch (epoch) whose CTAs have all left the
+   * loop; on a line of its own, away from the host-written words */
+  unsigned long long down;
+  unsigned long long pad2[7];
 };
 
 /* Device-side state. */
@@ -109,12 +113,14 @@ struct SDev {
   unsigned long long tail_mirror; /* last tail a CTA read from host memory   */
   unsigned int poll_lock;         /* one CTA at a time reads host memory     */
   int stop;                       /* the host's stop flag, as last read      */
+  unsigned long long last_active; /* globaltimer of the last mirrored request */
+  unsigned long long exited;      /* CTAs that left the loop, over all launches */
 };
 
 struct SArgs {
   const SReq *ring;
   SDone *done;
-  const SCtl *ctl;
+  SCtl *ctl;
   SDev *dev;
   unsigned int *tiles_done; /* per slot */
   unsigned long long *tctr; /* per slot: the claim word, set when the request is mirrored */
@@ -124,6 +130,8 @@ struct SArgs {
   uint64_t slice;
   int npes;
   unsigned long long idle_ns;
+  unsigned long long epoch; /* this launch's number, reported in ctl->down */
+  unsigned mirror_batch;    /* requests one poll copies at most */
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long *p) {
@@ -168,7 +176,12 @@ __device__ int read_req(const SArgs &a, unsigned long long r, SReq *out) {
   return vld(&m->seq) == r + 1 ? 1 : 0;
 }
 
-constexpr unsigned long long kMirrorBatch = kServeThreads / 16; /* requests one poll copies */
+/* Requests one poll copies at most (B200SHM_SERVE_MIRROR_BATCH overrides
+ * it).  The copy costs about one round trip to host memory whatever its
+ * size, so a saturated loop is bounded by batch / round trip: on the
+ * serving workload, saturated, 16 per poll served 0.78 M requests/s (1.09 M
+ * fetch-adds/s), 64 served 1.08 M (1.93 M), 256 served 1.16 M (2.29 M). */
+constexpr unsigned kMirrorBatch = 256;
 
 /* Claim the next tiles (thread 0).  Returns 1 with request *cr, tiles
  * [*ct, *ct + *count) and the request in *req; 2 when this CTA took the poll
@@ -203,7 +216,7 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
         if (*(const volatile int *)&a.ctl->stop) *(volatile int *)&a.dev->stop = 1;
         if (ht > mt) { /* the whole CTA copies them, still holding the lock */
           *mfrom = mt;
-          *mupto = ht < mt + kMirrorBatch ? ht : mt + kMirrorBatch;
+          *mupto = ht < mt + a.mirror_batch ? ht : mt + a.mirror_batch;
           *r_hint = r;
           return 2;
         }
@@ -214,7 +227,11 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
          * every waiting CTA on every turn floods the path to the host and
          * stalls every other memory access behind it */
         if (*(const volatile int *)&a.dev->stop) return 0;
-        if (now_ns() - idle_since > a.idle_ns) return 0;
+        /* idle is the loop's idle time, not this CTA's: a CTA that wins no
+         * claim for a while stays as long as requests keep arriving */
+        const unsigned long long act = vld(&a.dev->last_active), now = now_ns();
+        const unsigned long long since = act > idle_since ? act : idle_since;
+        if (now > since && now - since > a.idle_ns) return 0;
         __nanosleep(backoff);
         backoff = backoff < 512 ? backoff * 2 : 512;
       }
@@ -542,24 +559,36 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
   fence_gpu();
   __syncthreads();
   const unsigned long long now = now_ns();
-  for (unsigned w = threadIdx.x; w < n * 16; w += kServeThreads) {
-    const unsigned i = w >> 4, k = w & 15;
-    if (k == 14) continue;
-    const unsigned slot = (unsigned)((from + i) % a.Q);
-    const unsigned long long v =
-        k == 15 ? now : ((const volatile unsigned long long *)&a.ring[slot])[k];
-    ((volatile unsigned long long *)&a.mreq[slot])[k] = v;
+  /* the words of host memory four at a time per thread, all loads issued
+   * before the first store, so a batch costs about one round trip to the
+   * host rather than one per pass */
+  for (unsigned w0 = threadIdx.x; w0 < n * 16; w0 += 4 * kServeThreads) {
+    unsigned long long v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const unsigned w = w0 + j * kServeThreads, i = w >> 4, k = w & 15;
+      v[j] = 0;
+      if (w < n * 16 && k < 14)
+        v[j] = ((const volatile unsigned long long *)&a.ring[(from + i) % a.Q])[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const unsigned w = w0 + j * kServeThreads, i = w >> 4, k = w & 15;
+      if (w < n * 16 && k != 14)
+        ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[k] = k == 15 ? now : v[j];
+    }
   }
   fence_gpu();
   __syncthreads();
-  if (threadIdx.x < n) {
-    const unsigned long long x = from + threadIdx.x;
+  for (unsigned i = threadIdx.x; i < n; i += kServeThreads) {
+    const unsigned long long x = from + i;
     ((volatile unsigned long long *)&a.mreq[x % a.Q])[14] = x + 1;
   }
   fence_gpu();
   __syncthreads();
-  if (threadIdx.x < n) { /* the claim word last: it opens the request to claims */
-    const unsigned long long x = from + threadIdx.x;
+  for (unsigned i = threadIdx.x; i < n; i += kServeThreads) {
+    /* the claim word last: it opens the request to claims */
+    const unsigned long long x = from + i;
     const unsigned long long nt = ((const volatile unsigned long long *)&a.mreq[x % a.Q])[9];
     const unsigned long long k = share_tiles(nt, gridDim.x);
     atomicExch(&a.tctr[x % a.Q], claim_word(x, (nt + k - 1) / k));
@@ -567,6 +596,7 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
   fence_gpu();
   __syncthreads();
   if (threadIdx.x == 0) {
+    *(volatile unsigned long long *)&a.dev->last_active = now;
     *(volatile unsigned long long *)&a.dev->tail_mirror = upto;
     fence_gpu();
     atomicExch(&a.dev->poll_lock, 0u);
@@ -594,7 +624,16 @@ __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
       s_status = 0;
     }
     __syncthreads();
-    if (!s_go) return;
+    if (!s_go) {
+      if (threadIdx.x == 0) { /* the launch's last CTA out tells the host */
+        const unsigned long long out = atomicAdd(&a.dev->exited, 1ull) + 1;
+        if (out % gridDim.x == 0) {
+          fence_sys();
+          st_release_sys(&a.ctl->down, a.epoch);
+        }
+      }
+      return;
+    }
     if (s_go == 2) {
       mirror_ring(a, s_mfrom, s_mupto);
       idle_since = now_ns();
@@ -689,10 +728,22 @@ struct b200shm_server {
 namespace b200 {
 namespace {
 
-int ensure_running(b200shm_server *s) {
+/* A fault of the loop's kernel, if it had one (the loop is otherwise
+ * watched through host words only). */
+int stream_error(b200shm_server *s) {
   const cudaError_t e = cudaStreamQuery(s->stream);
-  if (e == cudaErrorNotReady) return B200SHM_OK;
-  if (e != cudaSuccess) return cuda_fail(e, "serving loop");
+  return e == cudaSuccess || e == cudaErrorNotReady ? B200SHM_OK : cuda_fail(e, "serving loop");
+}
+
+/* Relaunch the loop when its last launch has left (all of its CTAs have,
+ * or are about to: the new launch is ordered after them on the stream).
+ * One read of a host word, no driver call, while the loop runs. */
+int ensure_running(b200shm_server *s) {
+  if (s->args.epoch && *(const volatile unsigned long long *)&s->h_ctl->down != s->args.epoch)
+    return B200SHM_OK;
+  const cudaError_t e = cudaStreamQuery(s->stream);
+  if (e != cudaSuccess && e != cudaErrorNotReady) return cuda_fail(e, "serving loop");
+  s->args.epoch++;
   k_serve<<<s->ctas, kServeThreads, 0, s->stream>>>(s->args);
   count_launch();
   const cudaError_t le = cudaGetLastError();
@@ -874,6 +925,9 @@ int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
   a.slice = st().slice;
   a.npes = st().npes;
   a.idle_ns = (unsigned long long)(idle * 1e9);
+  a.mirror_batch = kMirrorBatch;
+  if (const char *mb = getenv("B200SHM_SERVE_MIRROR_BATCH"))
+    if (atoi(mb) > 0) a.mirror_batch = (unsigned)std::min(atoi(mb), 1024);
   int rc = ensure_running(s);
   if (rc) return bail(rc);
   *out = s;
@@ -912,7 +966,16 @@ int b200shm_serve_poll(b200shm_server *s, uint64_t ticket, uint64_t *fetched) {
   if (!s) return fail(B200SHM_ERR_ARG, "serve_poll: null server");
   const SDone *d = &s->h_done[ticket % s->Q];
   const unsigned long long seq = *(const volatile unsigned long long *)&d->seq;
-  if (seq < ticket + 1) return 0;
+  if (seq < ticket + 1) {
+    /* a loop that idled out right after this request was published is
+     * brought back here too (one read of a host word while it runs) */
+    if (*(const volatile unsigned long long *)&s->h_ctl->down == s->args.epoch) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      const int er = ensure_running(s);
+      if (er) return er;
+    }
+    return 0;
+  }
   std::atomic_thread_fence(std::memory_order_acquire);
   if (fetched) *fetched = *(const volatile unsigned long long *)&d->fetched;
   const int status = *(const volatile int *)&d->status;
@@ -936,14 +999,17 @@ int b200shm_serve_wait(b200shm_server *s, uint64_t ticket, double timeout_second
   for (unsigned it = 0;; it++) {
     const int rc = b200shm_serve_poll(s, ticket, fetched);
     if (rc) return rc < 0 ? rc : B200SHM_OK;
-    if ((it & 1023) == 1023) {
+    if ((it & 63) == 63) {
       std::lock_guard<std::mutex> lk(s->mu);
       const int er = ensure_running(s); /* the kernel may have idled out meanwhile */
       if (er) return er;
     }
-    if (host_now() - t0 > timeout_seconds)
+    if (host_now() - t0 > timeout_seconds) {
+      const int se = stream_error(s);
+      if (se) return se;
       return fail(B200SHM_ERR_TIMEOUT, "serve_wait: request %llu not complete after %.3f s",
                   (unsigned long long)ticket, timeout_seconds);
+    }
   }
 }
 
@@ -1049,14 +1115,17 @@ int b200shm_serve_replay(b200shm_server *s, const b200shm_request *reqs, uint64_
         i++;
       }
     }
-    if ((it & 4095) == 4095 && !pend.empty()) {
+    if ((it & 63) == 63 && !pend.empty()) {
       std::lock_guard<std::mutex> lk(s->mu);
       const int er = ensure_running(s);
       if (er) return er;
     }
-    if (host_now() - last_progress > 30.0)
+    if (host_now() - last_progress > 30.0) {
+      const int se = stream_error(s);
+      if (se) return se;
       return fail(B200SHM_ERR_TIMEOUT, "serve_replay: no progress for 30 s (%llu of %llu done)",
                   (unsigned long long)done, (unsigned long long)n);
+    }
   }
   return B200SHM_OK;
 }
