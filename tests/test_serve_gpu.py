@@ -232,3 +232,30 @@ def test_other_calls_do_not_wait_for_a_running_loop(B, heap):
         srv.stop()
     assert (B.get_rows(d, x[0].nbytes, np.int32, team=(0, 1, 4)) == x.sum(axis=0)).all()
     assert B.get_rows(d2, 4 * x[0].nbytes, np.uint8, team=(0, 1, 4))[1].tobytes() == x.tobytes()
+
+
+@pytest.mark.parametrize("batch", ["1", "1024"])
+def test_mirror_batch_sizes(B, heap, monkeypatch, batch):
+    """The mirror copies one request per poll, or up to 1024 (four passes of
+    the CTA per step): 3000 fetch-adds arriving at once on 8 counters add up
+    and hand out each counter's values exactly once."""
+    monkeypatch.setenv("B200SHM_SERVE_MIRROR_BATCH", batch)
+    NC = 8
+    ctr = heap(NC * 8)
+    B.memset(ctr, 0, NC * 8, team=(0, 1, 4))
+    rng = np.random.default_rng(int(batch))
+    items = [dict(kind="amo", op="fetch_add", dtype="int64", pe=int(rng.integers(4)),
+                  dest=ctr + 8 * int(rng.integers(NC)), value=1) for _ in range(3000)]
+    srv = B.Server(queue_slots=1024)
+    try:
+        _, fetched = srv.replay(B.make_requests(items), np.zeros(len(items)))
+    finally:
+        srv.stop()
+    seen = {}
+    for it, f in zip(items, fetched):
+        seen.setdefault((it["pe"], it["dest"]), []).append(int(f))
+    counters = B.get_rows(ctr, NC * 8, np.int64, team=(0, 1, 4))
+    for (pe, off), vals in seen.items():
+        assert sorted(vals) == list(range(len(vals)))
+        assert counters[pe, (off - ctr) // 8] == len(vals)
+    assert counters.sum() == len(items)
