@@ -265,14 +265,15 @@ typedef struct b200shm_request {
 
 typedef struct b200shm_server b200shm_server;
 
-/* Start the serving loop: a persistent kernel of `ctas` CTAs (0 = one per
- * SM) on its own stream that drains a ring of queue_slots requests kept in
- * mapped host memory.  Requests are cut into tiles that idle CTAs claim,
- * so a large request spreads over the GPU while small ones pass it; each
- * request reports completion through a word in host memory.  A CTA with no
- * published work for idle_seconds (0 = 0.25 s) exits; the host relaunches the
- * kernel when new work arrives, so the loop holds the GPU only while it is
- * used.  Replaces the reference's issue-one-call-and-wait model
+/* Start the serving loop: a persistent kernel of `ctas` CTAs (0 = two per
+ * SM, as many as fit at once) on its own stream that drains a ring of
+ * queue_slots requests kept in mapped host memory.  Requests are cut into
+ * tiles, and a request's tiles into at most one share per CTA, which idle
+ * CTAs claim, so a large request spreads over the GPU while small ones pass
+ * it; each request reports completion through a word in host memory.  When
+ * no new request has arrived for idle_seconds (0 = 0.25 s) the CTAs exit;
+ * the next enqueue, poll or wait relaunches the kernel, so the loop holds
+ * the GPU only while it is used.  Replaces the reference's issue-one-call-and-wait model
  * (shmem_* -> shcoll / shmemc_ctx_* round trips, src/shcoll/src/*.c,
  * src/shmemc/ucx/comms.c) for streams of small operations.  Requests in
  * flight together may run in any order and concurrently, as non-blocking
