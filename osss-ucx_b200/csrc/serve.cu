@@ -66,8 +66,32 @@ __host__ __device__ __forceinline__ unsigned long long share_tiles(unsigned long
                                                                    unsigned ctas) {
   return (ntiles + ctas - 1) / ctas;
 }
+/* Tile sizes.  A tile is one CTA's work, so a smaller tile finishes a large
+ * request sooner (and frees its ring slot sooner) at the cost of more
+ * claims.  Measured on the serving workload (200k requests/s offered, and
+ * the same stream saturated), reduce tiles reading 256 / 128 / 64 KiB:
+ * p99 67.5 / 48.5 / 40.7 us, saturated 1.17M / 1.15M / 1.10M requests/s;
+ * copy chunks of 16 KiB lost on both counts against 32 KiB. */
 constexpr uint64_t kCopyChunk = 32u << 10;       /* bytes per copy tile            */
-constexpr uint64_t kReduceTileRead = 256u << 10; /* source bytes per reduce tile   */
+constexpr uint64_t kReduceTileRead = 128u << 10; /* source bytes per reduce tile   */
+
+/* The tile sizes in force: the defaults above, or B200SHM_SERVE_COPY_CHUNK /
+ * B200SHM_SERVE_REDUCE_TILE (bytes, a multiple of 4 KiB from 4 KiB to
+ * 16 MiB), read once. */
+uint64_t tile_bytes(const char *var, uint64_t dflt) {
+  const char *e = getenv(var);
+  if (!e) return dflt;
+  const unsigned long long v = strtoull(e, nullptr, 0);
+  return v >= 4096 && v <= (16ull << 20) && v % 4096 == 0 ? v : dflt;
+}
+uint64_t copy_chunk() {
+  static const uint64_t v = tile_bytes("B200SHM_SERVE_COPY_CHUNK", kCopyChunk);
+  return v;
+}
+uint64_t reduce_tile_read() {
+  static const uint64_t v = tile_bytes("B200SHM_SERVE_REDUCE_TILE", kReduceTileRead);
+  return v;
+}
 
 /* A ring slot (mapped host memory, written by the host). */
 struct alignas(16) SReq {
@@ -784,7 +808,7 @@ int plan_request(const b200shm_request &r0, SReq *q) {
       return rc;
     if (r.dest_off != r.src_off && overlaps(r.dest_off, bytes, r.src_off, bytes))
       return fail(B200SHM_ERR_ARG, "serve: reduce dest and source overlap");
-    uint64_t unit = kReduceTileRead / ((uint64_t)r.pe_size * es);
+    uint64_t unit = reduce_tile_read() / ((uint64_t)r.pe_size * es);
     unit = (unit + kServeThreads - 1) / kServeThreads * kServeThreads;
     if (unit < kServeThreads) unit = kServeThreads;
     q->unit = unit;
@@ -841,13 +865,13 @@ int plan_request(const b200shm_request &r0, SReq *q) {
   default: return fail(B200SHM_ERR_ARG, "serve: request kind %d", r.kind);
   }
   if (q->nseg) { /* copy tiling */
-    q->unit = kCopyChunk;
-    if (r.n >= kCopyChunk) {
-      q->cps = (r.n + kCopyChunk - 1) / kCopyChunk;
+    q->unit = copy_chunk();
+    if (r.n >= copy_chunk()) {
+      q->cps = (r.n + copy_chunk() - 1) / copy_chunk();
       q->spt = 0;
       q->ntiles = q->nseg * q->cps;
     } else {
-      q->spt = r.n ? kCopyChunk / r.n : q->nseg;
+      q->spt = r.n ? copy_chunk() / r.n : q->nseg;
       if (q->spt < 1) q->spt = 1;
       q->ntiles = (q->nseg + q->spt - 1) / q->spt;
     }
