@@ -51,6 +51,7 @@ namespace b200 {
 namespace {
 
 constexpr int kServeThreads = 256;
+constexpr unsigned long long kStopBit = 1ull << 63;
 /* The claim word of a ring slot: [63:40] the request it serves (its low 24
  * bits), [39:24] the number of shares its tiles are cut into, [23:0] the
  * next share to hand out. */
@@ -122,14 +123,16 @@ static_assert(sizeof(SDone) == 64, "completion record of 64 bytes");
 
 /* Host-written control words (mapped host memory). */
 struct SCtl {
-  unsigned long long tail; /* requests published */
-  int stop;
-  int pad[13];
+  /* requests published, with kStopBit set once the host asked the loop to
+   * stop: one word, so a poll is one read of host memory */
+  unsigned long long tail;
+  unsigned long long pad[7];
   /* written by the device: the launch (epoch) whose CTAs have all left the
    * loop; on a line of its own, away from the host-written words */
   unsigned long long down;
   unsigned long long pad2[7];
 };
+static_assert(offsetof(SCtl, down) == 64 && sizeof(SCtl) == 128, "host and device lines apart");
 
 /* Device-side state. */
 struct SDev {
@@ -187,17 +190,14 @@ __device__ __forceinline__ void copy_words(SReq *dst, const SReq *src) {
 
 /* The device mirror of the ring: the CTA that holds the poll lock copies
  * newly published requests from host memory into it (sequence word last)
- * before it advances tail_mirror, so the other CTAs read requests from L2
- * only.  Read request r (< tail_mirror) into *out: 1 = a consistent copy,
- * 0 = the slot already holds a later request (so r is complete and all its
- * tiles were handed out). */
-__device__ int read_req(const SArgs &a, unsigned long long r, SReq *out) {
-  const SReq *m = &a.mreq[r % a.Q];
-  if (vld(&m->seq) != r + 1) return 0;
-  fence_gpu();
-  copy_words(out, m);
-  fence_gpu();
-  return vld(&m->seq) == r + 1 ? 1 : 0;
+ * before it opens them to claims, so the other CTAs read requests from L2
+ * only.  Copy request r into *out, for a CTA that holds a share of r (the
+ * caller has fenced after its claim): the slot keeps r until r completes,
+ * which needs that share, so one copy is consistent; 1 when the copy is of
+ * r (always, by that argument). */
+__device__ int copy_req(const SArgs &a, unsigned long long r, SReq *out) {
+  copy_words(out, &a.mreq[r % a.Q]);
+  return out->seq == r + 1 ? 1 : 0;
 }
 
 /* Requests one poll copies at most (B200SHM_SERVE_MIRROR_BATCH overrides
@@ -236,8 +236,9 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
       if (*(const volatile unsigned *)&a.dev->poll_lock == 0u &&
           atomicCAS(&a.dev->poll_lock, 0u, 1u) == 0u) {
         const unsigned long long mt = vld(&a.dev->tail_mirror);
-        const unsigned long long ht = ld_acquire_sys(&a.ctl->tail);
-        if (*(const volatile int *)&a.ctl->stop) *(volatile int *)&a.dev->stop = 1;
+        const unsigned long long hv = ld_acquire_sys(&a.ctl->tail);
+        if (hv & kStopBit) *(volatile int *)&a.dev->stop = 1;
+        const unsigned long long ht = hv & ~kStopBit;
         if (ht > mt) { /* the whole CTA copies them, still holding the lock */
           *mfrom = mt;
           *mupto = ht < mt + a.mirror_batch ? ht : mt + a.mirror_batch;
@@ -272,7 +273,7 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
       if (sh >= nsh) continue;
       /* share sh of request x is ours; x stays in its slot until it completes */
       fence_gpu();
-      if (req->seq != x + 1 && !read_req(a, x, req)) continue; /* not reached */
+      if (req->seq != x + 1 && !copy_req(a, x, req)) continue; /* not reached */
       const unsigned long long k = share_tiles(req->ntiles, gridDim.x);
       *cr = x;
       *ct = sh * k;
@@ -615,6 +616,7 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
     const unsigned long long x = from + i;
     const unsigned long long nt = ((const volatile unsigned long long *)&a.mreq[x % a.Q])[9];
     const unsigned long long k = share_tiles(nt, gridDim.x);
+    fence_gpu(); /* the whole request before its claim word, from this thread too */
     atomicExch(&a.tctr[x % a.Q], claim_word(x, (nt + k - 1) / k));
   }
   fence_gpu();
@@ -746,6 +748,7 @@ struct b200shm_server {
   int ctas = 0;
   cudaStream_t stream = nullptr;
   unsigned long long tail = 0; /* next ticket */
+  bool stopping = false;       /* stop asked: every tail written carries kStopBit */
   std::mutex mu;
 };
 
@@ -979,7 +982,7 @@ int b200shm_serve_enqueue(b200shm_server *s, const b200shm_request *req, uint64_
   std::atomic_thread_fence(std::memory_order_release);
   *(volatile unsigned long long *)&dst->seq = tk + 1;
   std::atomic_thread_fence(std::memory_order_release);
-  *(volatile unsigned long long *)&s->h_ctl->tail = tk + 1;
+  *(volatile unsigned long long *)&s->h_ctl->tail = (tk + 1) | (s->stopping ? kStopBit : 0);
   std::atomic_thread_fence(std::memory_order_seq_cst);
   s->tail = tk + 1;
   if (ticket) *ticket = tk;
@@ -1039,7 +1042,11 @@ int b200shm_serve_wait(b200shm_server *s, uint64_t ticket, double timeout_second
 
 int b200shm_serve_stop(b200shm_server *s) {
   if (!s) return B200SHM_OK;
-  *(volatile int *)&s->h_ctl->stop = 1;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+    *(volatile unsigned long long *)&s->h_ctl->tail = s->tail | kStopBit;
+  }
   std::atomic_thread_fence(std::memory_order_seq_cst);
   const double limit = (double)s->args.idle_ns * 1e-9 + 30.0, t0 = host_now();
   cudaError_t e;
