@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
         }
       } else {
         /* complete subtree of l1-l0 (a power of two) leaves: chunks of 8
-         * as fixed subtrees; LVL == 1: one chunk, LVL == 2: two chunks,
+         * as fixed subtrees; LVL == 1: one chunk, LVL == 2: two chunks, LVL == 4: four,
          * else a counter over the chunks (LVL levels hold 2^(LVL-1)) */
         const int n = l1 - l0;
         auto chunk = [&](int q0) {
@@ -312,6 +312,20 @@ __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
           for (int c2 = 0; c2 < 2; c2++) {
             const PK y = chunk(l0 + 8 * c2);
             r = c2 ? comb(r, y) : y;
+          }
+        } else if constexpr (LVL == 4) {
+          /* four chunks, one at a time: ((c0 c1)(c2 c3)) with two slots */
+          PK h, s2;
+#pragma unroll 1
+          for (int c4 = 0; c4 < 4; c4++) {
+            PK y = chunk(l0 + 8 * c4);
+            if (c4 & 1) {
+              y = comb(h, y);
+              if (c4 == 1) s2 = y;
+              else r = comb(s2, y);
+            } else {
+              h = y;
+            }
           }
         } else {
           PK stk[LVL];
@@ -428,15 +442,18 @@ void launch_coop_g(int lvl, bool pow2, uint64_t lanes, cudaStream_t s, const RAr
   } else if constexpr (ORDER == ORD_BINOMIAL) { /* only power-of-two teams get here */
     if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true>, lanes, s, a);
     else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true>, lanes, s, a);
+    else if (lvl == 4) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 4, true>, lanes, s, a);
     else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true>, lanes, s, a);
   } else {
     if (pow2) {
       if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, true>, lanes, s, a);
       else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, true>, lanes, s, a);
+      else if (lvl == 4) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 4, true>, lanes, s, a);
       else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, true>, lanes, s, a);
     } else {
       if (lvl == 1) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 1, false>, lanes, s, a);
       else if (lvl == 2) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 2, false>, lanes, s, a);
+      else if (lvl == 4) launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 4, false>, lanes, s, a);
       else launch_one(k_reduce_coop<T, OP, ORDER, V, G, MM, 7, false>, lanes, s, a);
     }
   }
@@ -464,14 +481,20 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
     if (a.nvec) {
       /* warp-cooperative split of the leaves is exact for any-order ops,
        * for butterflies, and for binomial trees over power-of-two teams.
-       * G lanes per column: 2 for chains, 4 for float trees (measured best
-       * on the 64-PE workload); B200SHM_REDUCE_COOP overrides (0 or 1 =
+       * G lanes per column: 2 for chains; for float trees as many as give
+       * each lane 32 leaves (2 to 8).  On the 64-PE workload G = 2 with
+       * 32 leaves per lane ran the f32 tree at 5.6-5.9 TB/s, G = 4 with 16
+       * at 5.2-5.4 (a warp then reads 128 rather than 256 consecutive bytes
+       * of each member per load).  B200SHM_REDUCE_COOP overrides (0 or 1 =
        * one lane per column). */
       constexpr bool any_order = ORDER == ORD_CHAIN && (std::is_integral<T>::value || MM);
       const int nleaves = ORDER == ORD_BUTTERFLY ? base.p2s : base.P;
       const bool splittable = any_order || ORDER == ORD_BUTTERFLY ||
                               (ORDER == ORD_BINOMIAL && (base.P & (base.P - 1)) == 0);
-      int G = ORDER == ORD_CHAIN ? 2 : 4;
+      /* float trees: 32 leaves per lane (four 8-leaf chunks, two slots),
+       * so G = 2 at 64 leaves; chains: G = 2 */
+      int G = 2;
+      if constexpr (ORDER != ORD_CHAIN) G = std::max(2, std::min(8, nleaves / 32));
       const char *ec = getenv("B200SHM_REDUCE_COOP");
       if (ec) G = atoi(ec);
       if (G < 1) G = 1;
@@ -484,7 +507,8 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
           const uint64_t lanes = a.nvec * (uint64_t)G;
           const int chunks = nleaves / G / 8; /* tree chunks per lane */
           const bool pow2 = ORDER != ORD_BUTTERFLY || base.P == base.p2s;
-          launch_coop<T, OP, ORDER, V, MM>(G, ORDER == ORD_CHAIN ? 1 : chunks <= 1 ? 1 : chunks == 2 ? 2 : 7,
+          launch_coop<T, OP, ORDER, V, MM>(G, ORDER == ORD_CHAIN ? 1 : chunks <= 1 ? 1 : chunks == 2 ? 2
+                                                 : chunks == 4 ? 4 : 7,
                                            pow2, lanes, s, a);
           count_launch();
           done += a.nvec * V;

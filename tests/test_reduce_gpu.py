@@ -66,7 +66,8 @@ def combos():
 @pytest.mark.parametrize("op,dt", combos())
 def test_reduce_matches_oracle(B, heap, rs, algo, op, dt):
     seed = zlib.crc32(f"{algo}{op}{dt}".encode()) & 0xFFFF
-    for P, N in [(1, 9), (2, 17), (3, 40), (5, 1), (8, 1000), (13, 77), (32, 131), (64, 257)]:
+    for P, N in [(1, 9), (2, 17), (3, 40), (5, 1), (8, 1000), (13, 77), (32, 131), (64, 257),
+                 (100, 45), (128, 37)]:
         x = gen.random_values(oracle.NP[dt], P, N, seed + P)
         if op == "prod" and dt.startswith("float"):
             x = (1.0 + 0.01 * x).astype(x.dtype)
