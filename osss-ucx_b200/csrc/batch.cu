@@ -799,12 +799,14 @@ void choose_plan(BDesc &d, bool tune, cudaStream_t s) {
       return;
     }
   }
-  /* heuristic default: 2 lanes for chains, 4 for trees (the per-call
-   * kernels' measured best), tiles of 1024 packs */
+  /* heuristic default: 2 lanes per column, tiles of 1024 packs.  Trees
+   * over more than 8 members at 2 lanes ran the batching workload in
+   * 2.62 ms, at 4 lanes 2.72 ms, at 8 lanes 3.09 ms (fewer, longer runs
+   * of each member per warp load). */
   /* small teams: columns per lane rather than lanes per column (a
    * butterfly over <= 8 members: lanes of 2 leaves each) */
   int G = order == ORD_CHAIN ? (d.P <= 8 ? 1 : 2)
-                             : (order == ORD_BUTTERFLY && d.P <= 8 ? (d.p2s > 2 ? d.p2s / 2 : 1) : 4);
+                             : (order == ORD_BUTTERFLY && d.P <= 8 ? (d.p2s > 2 ? d.p2s / 2 : 1) : 2);
   while (G > 1 && !lanes_ok(d, G)) G >>= 1;
   while (!lanes_ok(d, G) && G < 8) G <<= 1;
   d.G = G;
