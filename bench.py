@@ -622,6 +622,13 @@ def run_batch(args, world, rank, local):
 SERVE_KINDS = ["reduce", "fcollect", "alltoall", "put", "get", "amo"]
 
 
+def serve_ring_bytes(slice_bytes):
+    """Bytes per PE of the dest ring of the serving stream (the slice after
+    the source regions and counters, less 2 MiB)."""
+    ring0 = (2 * (16 << 20) + 4096 * 8 + 4095) // 4096 * 4096
+    return slice_bytes - ring0 - (2 << 20)
+
+
 def serve_workload(nreq, rate, seed=6, PS=256, slice_bytes=256 << 20, slots=256):
     """nreq requests with Poisson arrivals at `rate`/s: kind uniform over
     reduce/fcollect/alltoall/put/get/atomic, payload (bytes each PE
@@ -636,7 +643,8 @@ def serve_workload(nreq, rate, seed=6, PS=256, slice_bytes=256 << 20, slots=256)
     SRC, NCTR = 16 << 20, 4096
     src32, src64, ctr = 0, SRC, 2 * SRC
     ring0 = (ctr + NCTR * 8 + 4095) // 4096 * 4096
-    ring_bytes = slice_bytes - ring0 - (2 << 20)
+    ring_bytes = serve_ring_bytes(slice_bytes)
+    assert ring_bytes == slice_bytes - ring0 - (2 << 20)
     arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
     arrival -= arrival[0]
     payload = np.exp(rng.uniform(np.log(8), np.log(4 << 20), nreq)).astype(np.int64)
@@ -718,7 +726,10 @@ def run_serve(args, world, rank, local):
                 "p99_us": round(float(np.percentile(x, 99)) * 1e6, 2),
                 "p999_us": round(float(np.percentile(x, 99.9)) * 1e6, 2)}
 
-    srv = B.Server(queue_slots=SLOTS)
+    # admission by heap bytes: the heap the stream's requests write into is
+    # the dest ring of every PE; admitted, incomplete requests may hold all of it
+    budget = serve_ring_bytes(SL) * PS
+    srv = B.Server(queue_slots=SLOTS, heap_budget=budget)
     warm = min(2000, len(items))
     srv.replay(B.make_requests(items[:warm]), arrival[:warm])  # warm-up stream
     launches0 = B.launch_count()
@@ -749,7 +760,9 @@ def run_serve(args, world, rank, local):
                        "requests": len(items), "arrival": "Poisson", "rate_per_s": args.serve_rate,
                        "mix": "uniform over reduce/fcollect/alltoall/put/get/atomic",
                        "payload": "log-uniform [8 B, 4 MiB] received per PE",
-                       "dtypes": "int32/int64/float32/float64", "queue_slots": SLOTS},
+                       "dtypes": "int32/int64/float32/float64", "queue_slots": SLOTS,
+                       "admission": "by heap bytes written (device counter)",
+                       "heap_budget_bytes": budget},
             "served": {"latency_all": pct(lat), "latency_le_64KiB": pct(lat, small),
                        "ops_per_s": round(len(items) / last, 1),
                        "offered_per_s": round(len(items) / float(arrival[-1]), 1),

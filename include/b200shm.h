@@ -288,6 +288,17 @@ typedef struct b200shm_server b200shm_server;
  * loop, where that matters. */
 int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
                         b200shm_server **out);
+/* The same, with admission by symmetric-heap bytes: requests are opened to
+ * the GPU in arrival order only while the heap bytes that the admitted,
+ * incomplete ones write (over all their members: a reduction n*size*P, an
+ * fcollect or alltoall block*P*P, a put or get n, an atomic 8) stay within
+ * heap_budget (0 = no limit); a later request waits in the ring until
+ * completions free enough, and a request larger than the whole budget is
+ * refused at enqueue.  Accounting is on the device (one counter raised by
+ * the CTA that admits, lowered by the CTA that completes).  No reference
+ * counterpart: the reference runs each call to completion. */
+int b200shm_serve_start_budget(uint32_t queue_slots, int ctas, double idle_seconds,
+                               uint64_t heap_budget, b200shm_server **out);
 /* Validate and publish one request; *ticket identifies it.  Returns
  * B200SHM_ERR_BUSY when all queue slots hold requests not yet complete. */
 int b200shm_serve_enqueue(b200shm_server *srv, const b200shm_request *req,

@@ -77,6 +77,8 @@ def _load():
         "b200shm_fill_uniform": (ci, [ci, ci, ci, u64, ci, u64, u64, ctypes.c_double,
                                       ctypes.c_double, vp]),
         "b200shm_serve_start": (ci, [ctypes.c_uint32, ci, ctypes.c_double, ctypes.POINTER(vp)]),
+        "b200shm_serve_start_budget": (ci, [ctypes.c_uint32, ci, ctypes.c_double, u64,
+                                            ctypes.POINTER(vp)]),
         "b200shm_serve_enqueue": (ci, [vp, vp, ctypes.POINTER(u64)]),
         "b200shm_serve_poll": (ci, [vp, u64, ctypes.POINTER(u64)]),
         "b200shm_serve_wait": (ci, [vp, u64, ctypes.c_double, ctypes.POINTER(u64)]),
@@ -342,9 +344,12 @@ def make_requests(items):
 class Server:
     """The serving loop (b200shm_serve_start / enqueue / poll / wait / stop)."""
 
-    def __init__(self, queue_slots=1024, ctas=0, idle_seconds=0.25):
+    def __init__(self, queue_slots=1024, ctas=0, idle_seconds=0.25, heap_budget=0):
+        """heap_budget: symmetric-heap bytes that admitted, incomplete
+        requests may write at once (0 = no limit)."""
         h = ctypes.c_void_p()
-        _check(lib.b200shm_serve_start(queue_slots, ctas, idle_seconds, ctypes.byref(h)))
+        _check(lib.b200shm_serve_start_budget(queue_slots, ctas, idle_seconds, heap_budget,
+                                              ctypes.byref(h)))
         self.h = h
 
     def enqueue(self, req):

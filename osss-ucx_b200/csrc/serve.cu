@@ -62,6 +62,24 @@ __host__ __device__ __forceinline__ unsigned long long claim_word(unsigned long 
                                                                   unsigned long long nshares) {
   return ((r & kField24) << kTagShift) | (nshares << kShareShift);
 }
+/* The symmetric-heap bytes a request writes, over all the members it
+ * writes to: what admission by heap bytes accounts for. */
+__host__ __device__ __forceinline__ unsigned long long heap_bytes(const b200shm_request &r) {
+  const unsigned long long P = r.pe_size > 0 ? (unsigned long long)r.pe_size : 1ull;
+  switch (r.kind) {
+  case B200SHM_REQ_REDUCE: {
+    const bool w8 = r.dtype == B200SHM_I64 || r.dtype == B200SHM_U64 || r.dtype == B200SHM_F64;
+    return r.n * (w8 ? 8ull : 4ull) * P;
+  }
+  case B200SHM_REQ_FCOLLECT:
+  case B200SHM_REQ_ALLTOALL: return r.n * P * P;
+  case B200SHM_REQ_PUT:
+  case B200SHM_REQ_GET: return r.n;
+  default: return 8;
+  }
+}
+constexpr unsigned kMirrorMax = 1024; /* the largest mirror batch */
+
 /* tiles per share: at most one share per CTA */
 __host__ __device__ __forceinline__ unsigned long long share_tiles(unsigned long long ntiles,
                                                                    unsigned ctas) {
@@ -103,6 +121,8 @@ struct alignas(16) SReq {
   unsigned long long spt;    /* copies with small segments: segments per tile, else 0 */
   unsigned long long cps;    /* copies with large segments: chunks per segment */
   unsigned long long seq;    /* ticket + 1 once the slot holds the request; written last */
+  /* in the ring: the request's heap bytes (host-written, read by the
+   * mirror for admission); in the device copy: when it was mirrored */
   unsigned long long pad;
 };
 static_assert(sizeof(SReq) == 128, "ring slot of 128 bytes");
@@ -141,6 +161,7 @@ struct SDev {
   unsigned int poll_lock;         /* one CTA at a time reads host memory     */
   int stop;                       /* the host's stop flag, as last read      */
   unsigned long long last_active; /* globaltimer of the last mirrored request */
+  unsigned long long inflight;    /* heap bytes of admitted, incomplete requests */
   unsigned long long exited;      /* CTAs that left the loop, over all launches */
 };
 
@@ -159,6 +180,7 @@ struct SArgs {
   unsigned long long idle_ns;
   unsigned long long epoch; /* this launch's number, reported in ctl->down */
   unsigned mirror_batch;    /* requests one poll copies at most */
+  unsigned long long budget; /* heap bytes admitted requests may hold, 0 = no limit */
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long *p) {
@@ -578,7 +600,12 @@ __device__ __noinline__ void serve_copy(const SReq &q, uint64_t t, char *base, u
  * it).  The sequence word is cleared before the copy is written, so a late
  * reader of the slot's previous request sees the change. */
 __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned long long upto) {
-  const unsigned n = (unsigned)(upto - from);
+  unsigned n = (unsigned)(upto - from);
+  __shared__ unsigned long long s_bytes[kMirrorMax]; /* heap bytes per request (budget only) */
+  __shared__ unsigned s_admit;
+  /* a snapshot taken early, overlapping the copy: completions only lower
+   * the count meanwhile, so an early reading can only admit less */
+  const unsigned long long used = a.budget && threadIdx.x == 0 ? vld(&a.dev->inflight) : 0;
   for (unsigned i = threadIdx.x; i < n; i += kServeThreads)
     ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[14] = 0;
   fence_gpu();
@@ -593,7 +620,7 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
     for (int j = 0; j < 4; j++) {
       const unsigned w = w0 + j * kServeThreads, i = w >> 4, k = w & 15;
       v[j] = 0;
-      if (w < n * 16 && k < 14)
+      if (w < n * 16 && k != 14 && (k != 15 || a.budget))
         v[j] = ((const volatile unsigned long long *)&a.ring[(from + i) % a.Q])[k];
     }
 #pragma unroll
@@ -601,10 +628,28 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
       const unsigned w = w0 + j * kServeThreads, i = w >> 4, k = w & 15;
       if (w < n * 16 && k != 14)
         ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[k] = k == 15 ? now : v[j];
+      if (w < n * 16 && k == 15) s_bytes[i] = v[j];
     }
   }
   fence_gpu();
   __syncthreads();
+  if (a.budget) {
+    /* admission by heap bytes: the longest run of the batch, in arrival
+     * order, whose bytes fit beside those of the admitted requests not yet
+     * complete.  Only the poll-lock holder adds to the count and completions
+     * only lower it, so the check cannot overshoot.  The rest stay in the
+     * host ring for a later poll. */
+    if (threadIdx.x == 0) {
+      unsigned long long add = 0;
+      unsigned k = 0;
+      while (k < n && used + add + s_bytes[k] <= a.budget) add += s_bytes[k++];
+      if (add) atomicAdd(&a.dev->inflight, add);
+      s_admit = k;
+    }
+    __syncthreads();
+    n = s_admit;
+    upto = from + n;
+  }
   for (unsigned i = threadIdx.x; i < n; i += kServeThreads) {
     const unsigned long long x = from + i;
     ((volatile unsigned long long *)&a.mreq[x % a.Q])[14] = x + 1;
@@ -720,6 +765,8 @@ __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
         *(volatile unsigned long long *)&dn->t[2] = now_ns();
         *(volatile int *)&dn->status = s_status;
         st_release_sys(&dn->seq, r + 1);
+        if (a.budget) /* its heap bytes free for the next admissions, once complete */
+          atomicAdd(&a.dev->inflight, 0ull - heap_bytes(q.r));
       }
     }
     idle_since = now_ns();
@@ -895,6 +942,11 @@ extern "C" {
 
 int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
                         b200shm_server **out) {
+  return b200shm_serve_start_budget(queue_slots, ctas, idle_seconds, 0, out);
+}
+
+int b200shm_serve_start_budget(uint32_t queue_slots, int ctas, double idle_seconds,
+                               uint64_t heap_budget, b200shm_server **out) {
   if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
   if (!out) return fail(B200SHM_ERR_ARG, "serve_start: null argument");
   if (queue_slots < 1 || queue_slots > (1u << 20))
@@ -952,9 +1004,10 @@ int b200shm_serve_start(uint32_t queue_slots, int ctas, double idle_seconds,
   a.slice = st().slice;
   a.npes = st().npes;
   a.idle_ns = (unsigned long long)(idle * 1e9);
+  a.budget = heap_budget;
   a.mirror_batch = kMirrorBatch;
   if (const char *mb = getenv("B200SHM_SERVE_MIRROR_BATCH"))
-    if (atoi(mb) > 0) a.mirror_batch = (unsigned)std::min(atoi(mb), 1024);
+    if (atoi(mb) > 0) a.mirror_batch = (unsigned)std::min(atoi(mb), (int)kMirrorMax);
   int rc = ensure_running(s);
   if (rc) return bail(rc);
   *out = s;
@@ -966,6 +1019,9 @@ int b200shm_serve_enqueue(b200shm_server *s, const b200shm_request *req, uint64_
   SReq q;
   int rc = plan_request(*req, &q);
   if (rc) return rc;
+  if (s->args.budget && heap_bytes(q.r) > s->args.budget)
+    return fail(B200SHM_ERR_ARG, "serve: request of %llu heap bytes, above the server's budget of %llu",
+                (unsigned long long)heap_bytes(q.r), (unsigned long long)s->args.budget);
   std::lock_guard<std::mutex> lk(s->mu);
   const unsigned long long tk = s->tail;
   const unsigned slot = (unsigned)(tk % s->Q);
@@ -978,6 +1034,7 @@ int b200shm_serve_enqueue(b200shm_server *s, const b200shm_request *req, uint64_
   *(volatile unsigned long long *)&dst->seq = 0;
   std::atomic_thread_fence(std::memory_order_release);
   q.seq = 0;
+  q.pad = heap_bytes(q.r); /* for admission by heap bytes */
   memcpy(dst, &q, sizeof(SReq));
   std::atomic_thread_fence(std::memory_order_release);
   *(volatile unsigned long long *)&dst->seq = tk + 1;

@@ -259,3 +259,47 @@ def test_mirror_batch_sizes(B, heap, monkeypatch, batch):
         assert sorted(vals) == list(range(len(vals)))
         assert counters[pe, (off - ctr) // 8] == len(vals)
     assert counters.sum() == len(items)
+
+
+def test_admission_by_heap_bytes(B, heap, src_region):
+    """A server whose heap budget holds one 64 KiB put admits one request at
+    a time: each request is claimed on the device only after the previous
+    one completed; every put lands; a request above the budget is refused."""
+    nb = 64 << 10
+    items = [dict(kind="put", team=(k % 8, 1, 1), pe=(5 * k + 3) % 64, src=src_region + 4096 * k,
+                  dest=heap(nb), n=nb) for k in range(24)]
+    srv = B.Server(queue_slots=64, heap_budget=nb)
+    try:
+        srv.replay(B.make_requests(items), np.zeros(len(items)))
+        tr = [srv.trace(t) for t in range(len(items))]
+        with pytest.raises(B.B200Error):
+            srv.enqueue(B.make_requests([dict(items[0], n=2 * nb)])[0])
+    finally:
+        srv.stop()
+    for t in range(1, len(items)):
+        assert tr[t][1] >= tr[t - 1][2], t  # claimed after the previous one completed
+    for it in items:
+        got = B.get_rows(it["dest"], nb, np.uint8, team=(it["pe"], 1, 1))
+        want = B.get_rows(it["src"], nb, np.uint8, team=(it["team"][0], 1, 1))
+        assert got.tobytes() == want.tobytes()
+
+
+def test_heap_budget_mix_equals_unbudgeted(B, heap, src_region):
+    """The mixed stream through a server with a tight heap budget (1 MiB)
+    gives the bytes of the same stream through an unbudgeted one."""
+    rng = np.random.default_rng(9)
+    dests, items = [], []
+    for _ in range(120):
+        items.append(random_request(rng, src_region, dests, heap, max_bytes=8 << 10))
+    budget = 1 << 20  # each request here writes at most 128 KiB of heap
+    out = []
+    for hb in (budget, 0):
+        clear_dests(B, dests)
+        srv = B.Server(queue_slots=64, heap_budget=hb)
+        try:
+            srv.replay(B.make_requests(items), np.zeros(len(items)))
+        finally:
+            srv.stop()
+        out.append(read_dests(B, dests))
+    for k, (g, w) in enumerate(zip(*out)):
+        assert g == w, (k, items[k])
