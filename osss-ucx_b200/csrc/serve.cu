@@ -259,8 +259,11 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
           atomicCAS(&a.dev->poll_lock, 0u, 1u) == 0u) {
         const unsigned long long mt = vld(&a.dev->tail_mirror);
         const unsigned long long hv = ld_acquire_sys(&a.ctl->tail);
-        if (hv & kStopBit) *(volatile int *)&a.dev->stop = 1;
         const unsigned long long ht = hv & ~kStopBit;
+        /* a stop takes effect once every published request is in the
+         * mirror (with a heap budget some may still wait for room), so the
+         * loop drains before it exits */
+        if ((hv & kStopBit) && ht == mt) *(volatile int *)&a.dev->stop = 1;
         if (ht > mt) { /* the whole CTA copies them, still holding the lock */
           *mfrom = mt;
           *mupto = ht < mt + a.mirror_batch ? ht : mt + a.mirror_batch;

@@ -303,3 +303,19 @@ def test_heap_budget_mix_equals_unbudgeted(B, heap, src_region):
         out.append(read_dests(B, dests))
     for k, (g, w) in enumerate(zip(*out)):
         assert g == w, (k, items[k])
+
+
+def test_stop_drains_a_budgeted_loop(B, heap, src_region):
+    """Requests still waiting for heap room when the host stops the loop are
+    served before it exits: stop drains."""
+    nb = 64 << 10
+    items = [dict(kind="put", team=(k % 8, 1, 1), pe=(7 * k + 1) % 64, src=src_region + 8192 * k,
+                  dest=heap(nb), n=nb) for k in range(12)]
+    srv = B.Server(queue_slots=32, heap_budget=nb)
+    for r in B.make_requests(items):
+        srv.enqueue(r)
+    srv.stop()
+    for it in items:
+        got = B.get_rows(it["dest"], nb, np.uint8, team=(it["pe"], 1, 1))
+        want = B.get_rows(it["src"], nb, np.uint8, team=(it["team"][0], 1, 1))
+        assert got.tobytes() == want.tobytes()
