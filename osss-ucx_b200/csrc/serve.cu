@@ -758,7 +758,10 @@ __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
     if (threadIdx.x == 0) {
       const unsigned slot = (unsigned)(r % a.Q);
       fence_gpu();
-      if (atomicAdd(&a.tiles_done[slot], s_count) + (unsigned long long)s_count == q.ntiles) {
+      /* a CTA that claimed every tile of the request is its only finisher
+       * (most small requests): no count to keep */
+      if (s_count == q.ntiles ||
+          atomicAdd(&a.tiles_done[slot], s_count) + (unsigned long long)s_count == q.ntiles) {
         fence_sys();
         a.tiles_done[slot] = 0;
         SDone *dn = &a.done[slot];
