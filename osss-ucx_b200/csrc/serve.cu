@@ -283,7 +283,7 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
         const unsigned long long since = act > idle_since ? act : idle_since;
         if (now > since && now - since > a.idle_ns) return 0;
         __nanosleep(backoff);
-        backoff = backoff < 512 ? backoff * 2 : 512;
+        backoff = backoff < 256 ? backoff * 2 : 256;
       }
       continue;
     }
@@ -605,6 +605,7 @@ __device__ __noinline__ void serve_copy(const SReq &q, uint64_t t, char *base, u
 __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned long long upto) {
   unsigned n = (unsigned)(upto - from);
   __shared__ unsigned long long s_bytes[kMirrorMax]; /* heap bytes per request (budget only) */
+  __shared__ unsigned long long s_nt[kMirrorMax];    /* tiles per request, as copied */
   __shared__ unsigned s_admit;
   /* a snapshot taken early, overlapping the copy: completions only lower
    * the count meanwhile, so an early reading can only admit less */
@@ -632,6 +633,7 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
       if (w < n * 16 && k != 14)
         ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[k] = k == 15 ? now : v[j];
       if (w < n * 16 && k == 15) s_bytes[i] = v[j];
+      if (w < n * 16 && k == 9) s_nt[i] = v[j];
     }
   }
   fence_gpu();
@@ -662,7 +664,7 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
   for (unsigned i = threadIdx.x; i < n; i += kServeThreads) {
     /* the claim word last: it opens the request to claims */
     const unsigned long long x = from + i;
-    const unsigned long long nt = ((const volatile unsigned long long *)&a.mreq[x % a.Q])[9];
+    const unsigned long long nt = s_nt[i];
     const unsigned long long k = share_tiles(nt, gridDim.x);
     fence_gpu(); /* the whole request before its claim word, from this thread too */
     atomicExch(&a.tctr[x % a.Q], claim_word(x, (nt + k - 1) / k));
