@@ -283,7 +283,7 @@ __device__ int claim(const SArgs &a, SReq *req, unsigned long long *cr, unsigned
         const unsigned long long since = act > idle_since ? act : idle_since;
         if (now > since && now - since > a.idle_ns) return 0;
         __nanosleep(backoff);
-        backoff = backoff < 256 ? backoff * 2 : 256;
+        backoff = backoff < 128 ? backoff * 2 : 128;
       }
       continue;
     }
