@@ -22,10 +22,14 @@
  *  - the CTA that finishes a request's last tile writes its completion word
  *    (sequence, AMO old value, status) to host memory after a system-scope
  *    fence;
- *  - a CTA with no published work sleeps with a growing back-off; after the
- *    idle limit (or when the host asks it to stop) it exits, holding no
- *    claim, and the host relaunches the kernel when work arrives again.
- *    Every wait in the kernel is bounded by that limit.
+ *  - a CTA with no published work sleeps with a growing back-off (at most
+ *    128 ns); once the loop has had no new request for the idle limit, or
+ *    the host asked it to stop and every published request is mirrored, it
+ *    exits, holding no claim; the last CTA out tells the host through a
+ *    host word, and the host relaunches the kernel when work arrives again.
+ *    Every wait in the kernel is bounded by that limit;
+ *  - with a heap budget, the mirror opens requests to claims only while the
+ *    heap bytes of the admitted, incomplete ones fit the budget.
  *
  * Results equal the per-call entry points': a reduction combines in the
  * reference algorithm's exact order (a left fold where any order is exact,
