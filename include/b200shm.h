@@ -121,7 +121,11 @@ int b200shm_reduce_host(int op, int dtype, int algo, int pe_start, int pe_stride
  * runtime that owns every device allocation through its own pool, or code
  * that may not call cudaMalloc at all).  No counterpart in the reference.
  * It needs no b200shm_init and allocates nothing: member i's rows are the
- * caller's device buffers source + i*source_stride and dest + i*dest_stride.
+ * caller's device buffers source + i*source_stride and dest + i*dest_stride
+ * (the strides may differ).  The dest rows must be the source rows
+ * themselves (in place: dest == source, equal strides) or lie wholly apart
+ * from every source row; any other overlap is rejected with
+ * B200SHM_ERR_ARG.  Grids are sized for the current device.
  * Float MIN/MAX keeps its list of order-dependent elements in a file-scope
  * static device array (2 MiB + 256 bytes per GPU that loads the library,
  * held until exit), so float MIN/MAX is limited to 2^18 elements per
@@ -186,6 +190,27 @@ int b200shm_broadcast(int root, int pe_start, int pe_stride, int pe_size,
  * B200SHM_ERR_TIMEOUT if a member's wait ran out of budget. */
 int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size,
                     void *stream);
+
+/* Set the budget of every device-side barrier wait to `ns` nanoseconds
+ * (0 restores the default of 2 s); returns the previous budget.  The
+ * reference's waits (shmem_long_wait_until, src/shmemc/ucx/waituntil.c:
+ * 18-51) spin without bound; here a member that does not arrive within the
+ * budget turns the barrier into B200SHM_ERR_TIMEOUT. */
+uint64_t b200shm_set_wait_budget(uint64_t ns);
+
+/* Failure injection for failure-detection tests: barrier `algo` over the
+ * team with member `absent` never arriving (its PE context is not
+ * started).  Every wait that depends on it runs out of its budget, the call
+ * returns B200SHM_ERR_TIMEOUT with the flag lines cleared, and the team's
+ * next barrier works.  No reference counterpart (a missing PE hangs the
+ * reference's barrier_sync_helper_*, src/shcoll/src/barrier.c:56-266). */
+int b200shm_barrier_absent(int algo, int pe_start, int pe_stride, int pe_size, int absent,
+                           void *stream);
+
+/* Number of barrier flag words that are not zero (every barrier returns its
+ * flags to zero, as the reference returns pSync to SHMEM_SYNC_VALUE,
+ * src/shcoll/src/barrier.c:56-266); for tests of the recovery path. */
+int64_t b200shm_barrier_flags_nonzero(void);
 
 /* ---------------------------------------------------------------------- */
 /* batched reductions                                                      */

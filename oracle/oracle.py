@@ -62,10 +62,21 @@ def reduce_types(op, form="reduce"):
         TO_ALL_MINMAX if op in ("min", "max") else TO_ALL_ARITH)
 
 
+def reference_tree():
+    """The reference source tree: $REFERENCE_TREE, else a `reference`
+    directory beside this repository; None when neither exists."""
+    cand = os.environ.get("REFERENCE_TREE") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "reference")
+    return cand if os.path.isfile(os.path.join(cand, "src", "shcoll", "src", "reduce.c")) else None
+
+
 def build(reference=True):
-    """Compile the restatement (and, when the reference tree exists, _ref)."""
-    target = "all" if reference else "restatement"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    """Compile the restatement and, when the reference tree is found, _ref."""
+    tree = reference_tree() if reference else None
+    cmd = ["make", "-s", "-C", HERE, "all" if tree else "restatement"]
+    if tree:
+        cmd.append("REF=" + tree)
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a):

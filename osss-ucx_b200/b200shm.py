@@ -69,6 +69,9 @@ def _load():
         "b200shm_alltoalls": (ci, [ci, ci, ci, u64, u64, i64, i64, u64, u64, vp]),
         "b200shm_broadcast": (ci, [ci, ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_barrier": (ci, [ci, ci, ci, ci, vp]),
+        "b200shm_set_wait_budget": (u64, [u64]),
+        "b200shm_barrier_absent": (ci, [ci, ci, ci, ci, ci, vp]),
+        "b200shm_barrier_flags_nonzero": (i64, []),
         "b200shm_amo_batch": (ci, [ci, ci, u64, vp, vp, vp, vp, vp, vp]),
         "b200shm_batch_create": (ci, [vp, u64, ci, ctypes.POINTER(vp)]),
         "b200shm_batch_run": (ci, [vp, vp]),
@@ -238,6 +241,26 @@ def broadcast(root, dest, src, nbytes, team=None, stream=None):
 def barrier(algo="binomial_tree", team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_barrier(BARRIER_ALGOS.index(algo), start, stride, size, stream))
+
+
+def set_wait_budget(seconds):
+    """Budget of every device barrier wait (0 = the default 2 s); returns the
+    previous budget in seconds."""
+    return lib.b200shm_set_wait_budget(int(seconds * 1e9)) * 1e-9
+
+
+def barrier_absent(algo, absent, team=None, stream=None):
+    """Barrier with member `absent` never arriving (failure injection)."""
+    start, stride, size = _team(team)
+    return _check(lib.b200shm_barrier_absent(BARRIER_ALGOS.index(algo), start, stride, size,
+                                             absent, stream))
+
+
+def barrier_flags_nonzero():
+    n = lib.b200shm_barrier_flags_nonzero()
+    if n < 0:
+        _check(n)
+    return n
 
 
 def amo_batch(amo, dtype, nops, pe_dev, off_dev, value_dev=None, cond_dev=None,

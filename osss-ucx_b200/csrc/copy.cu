@@ -79,57 +79,99 @@ __global__ void __launch_bounds__(256) k_collect(const char *src0, char *dst0, u
 }
 
 /* alltoall: member j's dest[k*B + b] = member k's src[j*B + b].
- * blockIdx.y = pair index k*P + j; blockIdx.x strides over the block. */
+ * Pairs k*P + j are spread over blockIdx.y (grid-stride when there are more
+ * pairs than the grid's y extent); blockIdx.x strides over the block. */
 template <bool VEC>
 __global__ void __launch_bounds__(256) k_alltoall(const char *src0, char *dst0, uint64_t step,
                                                   int P, uint64_t B) {
-  const int k = blockIdx.y / P, j = blockIdx.y % P;
-  const char *src = src0 + (uint64_t)k * step + (uint64_t)j * B;
-  char *dst = dst0 + (uint64_t)j * step + (uint64_t)k * B;
+  const uint64_t pairs = (uint64_t)P * (uint64_t)P;
   const uint64_t n = VEC ? B / 16 : B;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if constexpr (VEC) {
-    /* four vectors in flight per thread */
-    for (; v + 3 * stride < n; v += 4 * stride) {
-      uint4 u0 = ld16(src + v * 16), u1 = ld16(src + (v + stride) * 16);
-      uint4 u2 = ld16(src + (v + 2 * stride) * 16), u3 = ld16(src + (v + 3 * stride) * 16);
-      st16(dst + v * 16, u0);
-      st16(dst + (v + stride) * 16, u1);
-      st16(dst + (v + 2 * stride) * 16, u2);
-      st16(dst + (v + 3 * stride) * 16, u3);
+  for (uint64_t pr = blockIdx.y; pr < pairs; pr += gridDim.y) {
+    const uint64_t k = pr / (uint64_t)P, j = pr % (uint64_t)P;
+    const char *src = src0 + k * step + j * B;
+    char *dst = dst0 + j * step + k * B;
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if constexpr (VEC) {
+      /* four vectors in flight per thread */
+      for (; v + 3 * stride < n; v += 4 * stride) {
+        uint4 u0 = ld16(src + v * 16), u1 = ld16(src + (v + stride) * 16);
+        uint4 u2 = ld16(src + (v + 2 * stride) * 16), u3 = ld16(src + (v + 3 * stride) * 16);
+        st16(dst + v * 16, u0);
+        st16(dst + (v + stride) * 16, u1);
+        st16(dst + (v + 2 * stride) * 16, u2);
+        st16(dst + (v + 3 * stride) * 16, u3);
+      }
+      for (; v < n; v += stride) st16(dst + v * 16, ld16(src + v * 16));
+    } else {
+      for (; v < n; v += stride) dst[v] = src[v];
     }
-    for (; v < n; v += stride) st16(dst + v * 16, ld16(src + v * 16));
-  } else {
-    for (; v < n; v += stride) dst[v] = src[v];
+  }
+}
+
+/* alltoall of small blocks (fewer words per pair than a CTA has threads):
+ * one thread per word of the flattened [pair][word] space, so a CTA spans
+ * many pairs instead of idling most of its threads on one. */
+template <class W>
+__global__ void __launch_bounds__(256) k_alltoall_flat(const char *src0, char *dst0,
+                                                       uint64_t step, int P, uint64_t nw) {
+  const uint64_t total = (uint64_t)P * (uint64_t)P * nw;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t pr = i / nw, w = i - pr * nw;
+    const uint64_t k = pr / (uint64_t)P, j = pr - k * (uint64_t)P;
+    ((W *)(dst0 + j * step))[k * nw + w] = ((const W *)(src0 + k * step))[j * nw + w];
   }
 }
 
 /* strided alltoall (alltoalls.c:39-50, 78-83): element t from member k to
  * member l: src_k[(l*n + t)*sst] -> dest_l[(k*n + t)*dst].
- * blockIdx.y = pair index k*P + l. */
+ * Pairs k*P + l over blockIdx.y, grid-stride as in k_alltoall. */
 template <class E>
 __global__ void __launch_bounds__(256) k_alltoalls(const char *src0, char *dst0, uint64_t step,
                                                    int P, uint64_t n, int64_t dst, int64_t sst) {
-  const int k = blockIdx.y / P, l = blockIdx.y % P;
-  const E *src = (const E *)(src0 + (uint64_t)k * step) + (uint64_t)l * n * (uint64_t)sst;
-  E *d = (E *)(dst0 + (uint64_t)l * step) + (uint64_t)k * n * (uint64_t)dst;
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (uint64_t)gridDim.x * blockDim.x)
-    d[t * (uint64_t)dst] = src[t * (uint64_t)sst];
+  const uint64_t pairs = (uint64_t)P * (uint64_t)P;
+  for (uint64_t pr = blockIdx.y; pr < pairs; pr += gridDim.y) {
+    const uint64_t k = pr / (uint64_t)P, l = pr % (uint64_t)P;
+    const E *src = (const E *)(src0 + k * step) + l * n * (uint64_t)sst;
+    E *d = (E *)(dst0 + l * step) + k * n * (uint64_t)dst;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (uint64_t)gridDim.x * blockDim.x)
+      d[t * (uint64_t)dst] = src[t * (uint64_t)sst];
+  }
+}
+
+/* strided alltoall with few elements per pair: one thread per element of
+ * the flattened [pair][element] space */
+template <class E>
+__global__ void __launch_bounds__(256) k_alltoalls_flat(const char *src0, char *dst0,
+                                                        uint64_t step, int P, uint64_t n,
+                                                        int64_t dst, int64_t sst) {
+  const uint64_t total = (uint64_t)P * (uint64_t)P * n;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t pr = i / n, t = i - pr * n;
+    const uint64_t k = pr / (uint64_t)P, l = pr - k * (uint64_t)P;
+    const E *src = (const E *)(src0 + k * step);
+    E *d = (E *)(dst0 + l * step);
+    d[(k * n + t) * (uint64_t)dst] = src[(l * n + t) * (uint64_t)sst];
+  }
 }
 
 /* strided alltoall with an element size that is not 1/2/4/8/16 bytes */
 __global__ void __launch_bounds__(256) k_alltoalls_bytes(const char *src0, char *dst0,
                                                          uint64_t step, int P, uint64_t n,
                                                          int64_t dst, int64_t sst, uint64_t es) {
-  const int k = blockIdx.y / P, l = blockIdx.y % P;
-  const char *src = src0 + (uint64_t)k * step + (uint64_t)l * n * (uint64_t)sst * es;
-  char *d = dst0 + (uint64_t)l * step + (uint64_t)k * n * (uint64_t)dst * es;
-  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n * es;
-       x += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t t = x / es, b = x % es;
-    d[t * (uint64_t)dst * es + b] = src[t * (uint64_t)sst * es + b];
+  const uint64_t pairs = (uint64_t)P * (uint64_t)P;
+  for (uint64_t pr = blockIdx.y; pr < pairs; pr += gridDim.y) {
+    const uint64_t k = pr / (uint64_t)P, l = pr % (uint64_t)P;
+    const char *src = src0 + k * step + l * n * (uint64_t)sst * es;
+    char *d = dst0 + l * step + k * n * (uint64_t)dst * es;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n * es;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+      const uint64_t t = x / es, b = x % es;
+      d[t * (uint64_t)dst * es + b] = src[t * (uint64_t)sst * es + b];
+    }
   }
 }
 
@@ -151,6 +193,11 @@ __global__ void __launch_bounds__(256) k_broadcast(const char *src, char *dst0, 
     }
   }
 }
+
+/* Pairs of an all-to-all beyond this many loop over blockIdx.y. */
+constexpr uint64_t kMaxGridY = 65535;
+/* Blocks of fewer words than this per pair take the flattened kernels. */
+constexpr uint64_t kFlatWords = 64;
 
 /* CTAs along x for a per-pair / per-member extent of n work items, so that
  * the whole grid is about `want` CTAs. */
@@ -240,17 +287,33 @@ int alltoall_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint6
   if (overlaps(dest_off, B * (uint64_t)P, src_off, B * (uint64_t)P))
     return fail(B200SHM_ERR_ARG, "alltoall: dest and source overlap");
   if (B == 0) return B200SHM_OK;
-  if ((uint64_t)P * (uint64_t)P > 65535)
-    return fail(B200SHM_ERR_UNSUPPORTED, "alltoall: more than 255 members");
   Members m = members(pe_start, pe_stride, P);
-  const bool vec = ((src_off | dest_off | B | m.step) & 15u) == 0;
-  const uint64_t n = vec ? B / 16 : B;
+  const char *sp = m.first + src_off;
+  char *dp = m.first + dest_off;
   const uint64_t pairs = (uint64_t)P * P;
-  dim3 grid(x_blocks(vec ? (n + 3) / 4 : n, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
+  const uint64_t bits = src_off | dest_off | B | m.step;
+  const uint64_t w = bits & 15 ? (bits & 7 ? (bits & 3 ? 1 : 4) : 8) : 16;
+  if (B / w < kFlatWords) {
+    /* small blocks: threads over the flattened [pair][word] space */
+    const uint64_t nw = B / w;
+    const unsigned g = grid_for(pairs * nw, 256, 8);
+    switch (w) {
+    case 16: k_alltoall_flat<uint4><<<g, 256, 0, s>>>(sp, dp, m.step, P, nw); break;
+    case 8: k_alltoall_flat<unsigned long long><<<g, 256, 0, s>>>(sp, dp, m.step, P, nw); break;
+    case 4: k_alltoall_flat<unsigned><<<g, 256, 0, s>>>(sp, dp, m.step, P, nw); break;
+    default: k_alltoall_flat<unsigned char><<<g, 256, 0, s>>>(sp, dp, m.step, P, nw); break;
+    }
+    count_launch();
+    return B200SHM_OK;
+  }
+  const bool vec = w == 16;
+  const uint64_t n = vec ? B / 16 : B;
+  const unsigned gy = (unsigned)(pairs < kMaxGridY ? pairs : kMaxGridY);
+  dim3 grid(x_blocks(vec ? (n + 3) / 4 : n, gy, 8ull * st().sm_count * 4), gy);
   if (vec)
-    k_alltoall<true><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, B);
+    k_alltoall<true><<<grid, 256, 0, s>>>(sp, dp, m.step, P, B);
   else
-    k_alltoall<false><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, B);
+    k_alltoall<false><<<grid, 256, 0, s>>>(sp, dp, m.step, P, B);
   count_launch();
   return B200SHM_OK;
 }
@@ -274,14 +337,27 @@ int alltoalls_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint
   if ((rc = check_extent(dest_off, dbytes, "alltoalls dest"))) return rc;
   if (overlaps(dest_off, dbytes, src_off, sbytes))
     return fail(B200SHM_ERR_ARG, "alltoalls: dest and source overlap");
-  if ((uint64_t)P * (uint64_t)P > 65535)
-    return fail(B200SHM_ERR_UNSUPPORTED, "alltoalls: more than 255 members");
   Members m = members(pe_start, pe_stride, P);
   const uint64_t pairs = (uint64_t)P * P;
-  dim3 grid(x_blocks(n, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
   const char *sp = m.first + src_off;
   char *dp = m.first + dest_off;
   const bool al = ((src_off | dest_off | m.step) % es) == 0;
+  const bool typed = es == 1 || (al && (es == 2 || es == 4 || es == 8 || es == 16));
+  if (typed && n < kFlatWords) {
+    /* few elements per pair: threads over the flattened [pair][element] space */
+    const unsigned g = grid_for(pairs * n, 256, 8);
+    switch (es) {
+    case 8: k_alltoalls_flat<uint64_t><<<g, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst); break;
+    case 4: k_alltoalls_flat<uint32_t><<<g, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst); break;
+    case 2: k_alltoalls_flat<uint16_t><<<g, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst); break;
+    case 16: k_alltoalls_flat<uint4><<<g, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst); break;
+    default: k_alltoalls_flat<uint8_t><<<g, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst); break;
+    }
+    count_launch();
+    return B200SHM_OK;
+  }
+  const unsigned gy = (unsigned)(pairs < kMaxGridY ? pairs : kMaxGridY);
+  dim3 grid(x_blocks(n, gy, 8ull * st().sm_count * 4), gy);
   if (al && es == 8)
     k_alltoalls<uint64_t><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
   else if (al && es == 4)
@@ -293,7 +369,7 @@ int alltoalls_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint
   else if (al && es == 16)
     k_alltoalls<uint4><<<grid, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst);
   else {
-    dim3 g2(x_blocks(n * es, pairs, 8ull * st().sm_count * 4), (unsigned)pairs);
+    dim3 g2(x_blocks(n * es, gy, 8ull * st().sm_count * 4), gy);
     k_alltoalls_bytes<<<g2, 256, 0, s>>>(sp, dp, m.step, P, n, dst, sst, es);
   }
   count_launch();

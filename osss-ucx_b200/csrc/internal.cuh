@@ -83,11 +83,15 @@ inline bool overlaps(uint64_t a, uint64_t na, uint64_t b, uint64_t nb) {
   return na && nb && a < b + nb && b < a + na;
 }
 
+/* SMs that grids are sized for: the engine's device once b200shm_init has
+ * run, else the current device (entry points that need no init). */
+int grid_sms();
+
 /* Grid size for a grid-stride kernel: enough CTAs to cover `items` work
  * items with `threads` per CTA, capped at `per_sm` resident CTAs per SM. */
 inline unsigned grid_for(uint64_t items, int threads, int per_sm) {
   uint64_t need = (items + (uint64_t)threads - 1) / (uint64_t)threads;
-  uint64_t cap = (uint64_t)st().sm_count * (uint64_t)per_sm;
+  uint64_t cap = (uint64_t)grid_sms() * (uint64_t)per_sm;
   if (need < 1) need = 1;
   return (unsigned)(need < cap ? need : cap);
 }

@@ -390,7 +390,7 @@ unsigned reduce_grid(K kernel, int &occ, uint64_t nvec, int threads) {
     occ = o;
   }
   const uint64_t need = (nvec + threads - 1) / threads;
-  const uint64_t cap = (uint64_t)st().sm_count * (uint64_t)occ;
+  const uint64_t cap = (uint64_t)grid_sms() * (uint64_t)occ;
   return (unsigned)(need < cap ? (need ? need : 1) : cap);
 }
 
@@ -530,7 +530,7 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
     count_launch();
   }
   if constexpr (MM) {
-    k_minmax_fix<T, OP><<<2 * st().sm_count, 256, 0, s>>>(base, base.fix_list, base.fix_count,
+    k_minmax_fix<T, OP><<<2 * grid_sms(), 256, 0, s>>>(base, base.fix_list, base.fix_count,
                                                          base.fix_cap);
     count_launch();
   }
@@ -834,17 +834,20 @@ extern "C" int b200shm_reduce_host(int op, int dtype, int algo, int pe_start, in
  * device memory.
  *
  * Some callers of this code cannot call cudaMalloc: a host runtime that
- * owns all device memory through its own pool, code running inside a
- * captured or otherwise allocation-restricted region, or an embedding that
- * hands the engine pre-registered buffers and forbids it any allocation of
- * its own.  They cannot use b200shm_reduce either, because that needs the
- * arena and the deferred-element list that b200shm_init allocates.  This
- * entry point takes caller-owned device buffers directly and allocates
- * nothing: the one piece of scratch the reduction needs -- the list of
- * float MIN/MAX elements whose result depends on operand order (NaN, or
- * both +0 and -0, among the inputs), plus its counter and a status word --
- * lives in the file-scope array below, which every GPU that loads this
- * library holds until the process exits.
+ * owns all device memory through its own pool and hands out only buffers it
+ * has already placed, or an embedding that registers its buffers up front
+ * and forbids the library any allocation of its own.  They cannot use
+ * b200shm_reduce either, because that needs the arena and the
+ * deferred-element list that b200shm_init allocates.  This entry point
+ * takes caller-owned device buffers directly and allocates nothing: the one
+ * piece of scratch the reduction needs -- the list of float MIN/MAX
+ * elements whose result depends on operand order (NaN, or both +0 and -0,
+ * among the inputs), plus its counter and a status word -- lives in the
+ * file-scope array below, which every GPU that loads this library holds
+ * until the process exits.  The first call on a device resolves the
+ * array's device address (set-up, once per device); that first call should
+ * come before any stream capture.  Every call blocks until its result is
+ * in every dest.
  * ------------------------------------------------------------------------- */
 namespace b200 {
 
@@ -886,17 +889,31 @@ extern "C" int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, voi
   if (dest == nullptr || source == nullptr)
     return fail(B200SHM_ERR_ARG, "reduce_noalloc: null buffer");
   const uint64_t es = (uint64_t)kDtypeSize[dtype];
+  if (nelems > UINT64_MAX / es)
+    return fail(B200SHM_ERR_ARG, "reduce_noalloc: nelems %llu overflows the row size",
+                (unsigned long long)nelems);
   const uint64_t bytes = nelems * es;
   if (npes > 1 && (dest_stride < bytes || source_stride < bytes))
     return fail(B200SHM_ERR_ARG, "reduce_noalloc: member stride smaller than the %llu-byte row",
                 (unsigned long long)bytes);
-  if (dest != source) {
-    /* a member's dest row must not overlap its source row unless the two
-     * are the same buffer (in place), as for b200shm_reduce */
-    const char *d0 = (const char *)dest, *s0 = (const char *)source;
-    if (dest_stride == source_stride && d0 < s0 + bytes && s0 < d0 + bytes)
-      return fail(B200SHM_ERR_ARG, "reduce_noalloc: dest and source overlap without being identical");
-  }
+  /* the spans every member's rows cover: [buf, buf + (npes-1)*stride + bytes) */
+  const uint64_t rows = (uint64_t)(npes - 1);
+  if ((rows && (dest_stride > (UINT64_MAX - bytes) / rows ||
+                source_stride > (UINT64_MAX - bytes) / rows)))
+    return fail(B200SHM_ERR_ARG, "reduce_noalloc: member strides overflow the address space");
+  const uint64_t dspan = rows * dest_stride + bytes, sspan = rows * source_stride + bytes;
+  const uint64_t d0 = (uint64_t)(uintptr_t)dest, s0 = (uint64_t)(uintptr_t)source;
+  if (d0 > UINT64_MAX - dspan || s0 > UINT64_MAX - sspan)
+    return fail(B200SHM_ERR_ARG, "reduce_noalloc: buffer span wraps the address space");
+  /* The kernels read every member's source row of a column while other
+   * CTAs write dest rows, and the float MIN/MAX replay reads the sources
+   * after the dests of other elements are written: so the dest rows and the
+   * source rows must be either the very same rows (in place: same base,
+   * same stride) or fully apart. */
+  const bool in_place = d0 == s0 && (dest_stride == source_stride || npes == 1);
+  if (!in_place && overlaps(d0, dspan, s0, sspan))
+    return fail(B200SHM_ERR_ARG,
+                "reduce_noalloc: dest rows and source rows overlap without being the same rows");
   const bool minmax_float = (op == B200SHM_MIN || op == B200SHM_MAX) &&
                             (dtype == B200SHM_F32 || dtype == B200SHM_F64);
   if (minmax_float && nelems > kNoAllocMaxDeferred)

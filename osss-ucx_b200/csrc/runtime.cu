@@ -67,6 +67,25 @@ int finish(void *stream_arg, const char *what) {
   return B200SHM_OK;
 }
 
+int grid_sms() {
+  if (st().up) return st().sm_count;
+  static std::atomic<int> sms[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    (void)cudaGetLastError();
+    return st().sm_count;
+  }
+  int n = sms[dev].load(std::memory_order_relaxed);
+  if (n == 0) {
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+      (void)cudaGetLastError();
+      return st().sm_count;
+    }
+    sms[dev].store(n, std::memory_order_relaxed);
+  }
+  return n;
+}
+
 int check_team(int pe_start, int pe_stride, int pe_size) {
   if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
   if (pe_size < 1) return fail(B200SHM_ERR_ARG, "team size %d < 1", pe_size);

@@ -17,9 +17,16 @@
  */
 #include <stdint.h>
 
+#include <atomic>
+#include <vector>
+
 #include "internal.cuh"
 
 namespace b200 {
+
+/* default budget of a barrier wait: 2 s */
+constexpr long long kDefaultWaitBudgetNs = 2000000000ll;
+
 namespace {
 
 struct BArgs {
@@ -28,6 +35,7 @@ struct BArgs {
   int pe_start, pe_stride, P, algo;
   int *status;
   long long budget_ns;
+  int absent;      /* member that never arrives (failure injection), or -1 */
 };
 
 __device__ __forceinline__ unsigned long long *flag(const BArgs &a, int member, int round) {
@@ -123,7 +131,7 @@ __device__ void tree_barrier(const BArgs &a, int me, int parent, const int *ch, 
 
 __global__ void k_barrier(const BArgs a) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= a.P) return;
+  if (me >= a.P || me == a.absent) return;
   const long long deadline = now_ns() + a.budget_ns;
   const int P = a.P;
   int ch[32];
@@ -171,7 +179,10 @@ __global__ void k_barrier(const BArgs a) {
 
 }  // namespace
 
-int barrier_launch(int algo, int pe_start, int pe_stride, int P, cudaStream_t s) {
+/* budget of every barrier wait, ns (b200shm_set_wait_budget) */
+static std::atomic<long long> g_wait_budget_ns{kDefaultWaitBudgetNs};
+
+int barrier_launch(int algo, int pe_start, int pe_stride, int P, cudaStream_t s, int absent) {
   int rc = check_team(pe_start, pe_stride, P);
   if (rc) return rc;
   if (algo < 0 || algo >= B200SHM_BAR_NALGO)
@@ -189,7 +200,8 @@ int barrier_launch(int algo, int pe_start, int pe_stride, int P, cudaStream_t s)
   a.P = P;
   a.algo = algo;
   a.status = st().d_status;
-  a.budget_ns = 2000000000ll;
+  a.budget_ns = g_wait_budget_ns.load(std::memory_order_relaxed);
+  a.absent = absent;
   const int threads = P < 256 ? P : 256;
   const int blocks = (P + threads - 1) / threads;
   int per_sm = 0;
@@ -210,16 +222,54 @@ int barrier_reset_flags(cudaStream_t s) {
   return B200SHM_OK;
 }
 
-}  // namespace b200
-
-extern "C" int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size, void *stream) {
-  cudaStream_t s = b200::pick_stream(stream);
-  int rc = b200::barrier_launch(algo, pe_start, pe_stride, pe_size, s);
+/* One barrier, blocking or stream-ordered; a timed-out barrier leaves its
+ * flag lines cleared before it returns. */
+static int barrier_call(int algo, int pe_start, int pe_stride, int pe_size, int absent,
+                        void *stream, const char *what) {
+  cudaStream_t s = pick_stream(stream);
+  int rc = barrier_launch(algo, pe_start, pe_stride, pe_size, s, absent);
   if (rc) return rc;
-  rc = b200::finish(stream, "b200shm_barrier");
+  rc = finish(stream, what);
   if (rc == B200SHM_ERR_TIMEOUT) {
-    b200::barrier_reset_flags(s);
+    barrier_reset_flags(s);
     cudaStreamSynchronize(s);
   }
   return rc;
 }
+
+}  // namespace b200
+
+extern "C" {
+
+int b200shm_barrier(int algo, int pe_start, int pe_stride, int pe_size, void *stream) {
+  return b200::barrier_call(algo, pe_start, pe_stride, pe_size, -1, stream, "b200shm_barrier");
+}
+
+uint64_t b200shm_set_wait_budget(uint64_t ns) {
+  const long long v = ns == 0 ? b200::kDefaultWaitBudgetNs
+                              : (long long)(ns > (uint64_t)INT64_MAX / 2 ? (uint64_t)INT64_MAX / 2 : ns);
+  return (uint64_t)b200::g_wait_budget_ns.exchange(v);
+}
+
+int b200shm_barrier_absent(int algo, int pe_start, int pe_stride, int pe_size, int absent,
+                           void *stream) {
+  if (absent < 0 || absent >= pe_size)
+    return b200::fail(B200SHM_ERR_ARG, "barrier_absent: member %d is not in the team", absent);
+  return b200::barrier_call(algo, pe_start, pe_stride, pe_size, absent, stream,
+                            "b200shm_barrier_absent");
+}
+
+int64_t b200shm_barrier_flags_nonzero(void) {
+  using namespace b200;
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  const uint64_t words = (uint64_t)st().npes * (uint64_t)st().flag_rounds * 8ull;
+  std::vector<unsigned long long> h(words);
+  B200_CK(cudaStreamSynchronize(st().stream));
+  B200_CK(cudaMemcpy(h.data(), st().flags, words * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost));
+  int64_t n = 0;
+  for (unsigned long long w : h) n += w != 0;
+  return n;
+}
+
+}  // extern "C"

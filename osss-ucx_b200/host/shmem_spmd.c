@@ -88,6 +88,7 @@ typedef struct agg {
   void *outp, *outq;
   uint64_t *counts; /* collect: each member's own byte count, by team index */
   int counts_cap;
+  char msg[512];    /* the failure of the last launch, for every member */
 } agg_t;
 
 typedef struct b200_team {
@@ -199,10 +200,14 @@ static int arrive(b200_team_t *t, const coll_t *mine) {
     if (g->counts_cap >= t->size) g->counts[team_index(t, t_pe)] = mine->n;
   }
   if (++g->arrived == t->size) {
+    t_err[0] = 0;
     g->rc = g->mismatch ? set_err(B200SHM_ERR_ARG,
                                   "members passed different arguments (non-symmetric "
                                   "addresses or counts)")
                         : launch(t, g);
+    /* every member reports the same failure, whichever thread launched */
+    if (g->rc) snprintf(g->msg, sizeof(g->msg), "%s", t_err[0] ? t_err : b200shm_last_error());
+    else g->msg[0] = 0;
     g->arrived = 0;
     g->gen++;
     pthread_cond_broadcast(&g->cv);
@@ -210,9 +215,9 @@ static int arrive(b200_team_t *t, const coll_t *mine) {
     while (gen == g->gen) pthread_cond_wait(&g->cv, &g->mu);
   }
   const int rc = g->rc;
+  if (rc) set_err(rc, "%s", g->msg);
   pthread_mutex_unlock(&g->mu);
   t_status = rc;
-  if (rc && !t_err[0]) set_err(rc, "%s", b200shm_last_error());
   return rc;
 }
 

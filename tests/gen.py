@@ -53,3 +53,18 @@ def config1_inputs(npes=8, n_reduce=1024, n_fc=256, master=0xC0FFEE):
     x = uniform_int(np.int32, npes, n_reduce, master, -1000, 1000)
     fc = (np.arange(npes, dtype=np.int64)[:, None] << 32) | np.arange(n_fc, dtype=np.int64)[None, :]
     return x, fc
+
+
+def special_minmax(dtype, npes, n, seed):
+    """Floats where MIN/MAX depend on operand order: N(0,1) values with
+    about 1/5 each +0 and -0, and 10 % NaNs with distinct payloads."""
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((npes, n)).astype(dtype)
+    pick = rng.integers(0, 5, size=(npes, n))
+    x[pick == 0] = 0.0
+    x[pick == 1] = -0.0
+    m = rng.random((npes, n)) < 0.1
+    x[m] = np.nan
+    bits = x.view(np.uint32 if np.dtype(dtype).itemsize == 4 else np.uint64)
+    bits[m] |= rng.integers(1, 1 << 20, size=m.sum()).astype(bits.dtype)
+    return x

@@ -211,3 +211,83 @@ def test_restatement_matches_reference_collect(rs, ref, algo):
                     a=a, b=b)
             want = rs.collect(x, [c * 8 for c in counts], sum(counts) * 8 + 8)
             assert out.tobytes() == want.tobytes(), (algo, P, "team")
+
+
+# ---------------------------------------------------------------------------
+# the restatement against the reference at the team sizes and shapes the
+# GPU is run at (deeper butterflies, extra-PE folds of large teams, the
+# configured element counts)
+# ---------------------------------------------------------------------------
+LARGE_TEAMS = (16, 33, 64, 100, 128, 255, 256)
+
+
+@pytest.mark.parametrize("P", LARGE_TEAMS)
+def test_restatement_matches_reference_large_teams(rs, ref, P):
+    """Every (algorithm, op) at P members, three type-table entries each
+    (drawn per P), element counts on both sides of the Rabenseifner block
+    boundaries (N < p2s, N not a multiple of p2s)."""
+    rng = np.random.default_rng(1000 + P)
+    for algo in oracle.ALGOS:
+        for op in oracle.OPS:
+            names = list(oracle.reduce_types(op))
+            for tname in rng.choice(names, size=3, replace=False):
+                dt = oracle.SHMEM_TYPES[tname]
+                if algo == "binomial" and dt.startswith(("float", "complex")):
+                    continue  # arrival-order dependent in the reference
+                N = int(rng.choice([int(rng.integers(1, P)), int(rng.integers(P, 4 * P + 7))]))
+                x = gen.random_values(oracle.NP[dt], P, N, int(rng.integers(1 << 30)))
+                got = rs.reduce(algo, op, x)
+                want, _ = ref.reduce(algo, op, x, tname=str(tname))
+                assert value_bytes(got) == value_bytes(want), (algo, op, tname, P, N)
+
+
+@pytest.mark.parametrize("P", (100, 128, 255, 256))
+def test_restatement_matches_reference_special_minmax_large(rs, ref, P):
+    """NaN and mixed-sign zeros at large P: rec_dbl leaves member-dependent
+    bits, Rabenseifner block-dependent bits; both must match per member."""
+    for dt, tname in ((np.float32, "float"), (np.float64, "double")):
+        x = gen.special_minmax(dt, P, 3 * P + 5, P)
+        for algo in ("rec_dbl", "rabenseifner", "rabenseifner2", "linear"):
+            for op in ("min", "max"):
+                want, _ = ref.reduce(algo, op, x, tname=tname)
+                assert rs.reduce(algo, op, x).tobytes() == want.tobytes(), (algo, op, tname, P)
+
+
+def test_restatement_matches_reference_config2_shape(rs, ref):
+    """The headline shape itself: 64 members x 2^20 elements, f32 SUM
+    N(0,1) in all three butterfly orders, f64 MAX U(+-1e6), i64 XOR."""
+    P, N = 64, 1 << 20
+    f32 = gen.normal(np.float32, P, N, 1)
+    for algo in ("rec_dbl", "rabenseifner", "rabenseifner2"):
+        want, _ = ref.reduce(algo, "sum", f32)
+        assert rs.reduce(algo, "sum", f32).tobytes() == want.tobytes(), algo
+    f64 = gen.uniform(np.float64, P, N, 2, -1e6, 1e6)
+    want, _ = ref.reduce("rabenseifner", "max", f64)
+    assert rs.reduce("rabenseifner", "max", f64).tobytes() == want.tobytes()
+    i64 = gen.uniform_int(np.int64, P, N, 3)
+    want, _ = ref.reduce("rec_dbl", "xor", i64)
+    assert rs.reduce("rec_dbl", "xor", i64).tobytes() == want.tobytes()
+
+
+def test_restatement_matches_reference_config3_shape(rs, ref):
+    """The data-movement shapes at 128 members: fcollect64 of 4096 int64
+    (the default bruck_inplace), alltoallmem of 64 KiB blocks and alltoalls64
+    with dst 2, sst 3 over 4096 elements per pair (shift_exchange_barrier)."""
+    P = 128
+    x = gen.uniform_int(np.int64, P, 4096, 1)
+    out = np.zeros((P, P * 4096), np.int64)
+    ref.run(oracle.K_SIZED, "shcoll_fcollect64_bruck_inplace", x, out, nelems=4096)
+    assert rs.fcollect(x).tobytes() == out.tobytes()
+    x = gen.uniform_int(np.uint8, P, P * 65536, 2)
+    out = np.zeros_like(x)
+    ref.run(oracle.K_TEAM_COPY, "shcoll_alltoallmem_shift_exchange_barrier", x, out,
+            nelems=65536)
+    assert rs.alltoall(x).tobytes() == out.tobytes()
+    del x, out
+    n = 4096
+    x = gen.uniform_int(np.int64, P, P * n * 3, 3)
+    d0 = gen.uniform_int(np.int64, P, P * n * 2, 4)
+    out = d0.copy()
+    ref.run(oracle.K_ALLTOALLS_SIZED, "shcoll_alltoalls64_shift_exchange_barrier", x, out,
+            nelems=n, a=2, b=3)
+    assert rs.alltoalls(x, d0, 2, 3, n).tobytes() == out.tobytes()

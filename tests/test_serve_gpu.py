@@ -319,3 +319,26 @@ def test_stop_drains_a_budgeted_loop(B, heap, src_region):
         got = B.get_rows(it["dest"], nb, np.uint8, team=(it["pe"], 1, 1))
         want = B.get_rows(it["src"], nb, np.uint8, team=(it["team"][0], 1, 1))
         assert got.tobytes() == want.tobytes()
+
+
+def test_wait_on_a_ticket_that_never_completes_times_out(B, heap):
+    """The host-side bound: waiting on a ticket that was never issued (so it
+    never completes) returns B200SHM_ERR_TIMEOUT after the timeout, and the
+    server keeps serving afterwards."""
+    a = heap(4096)
+    B.memset(a, 0, 8, team=(0, 1, 1))
+    srv = B.Server(queue_slots=8, idle_seconds=0.05)
+    try:
+        req = B.make_requests([dict(kind="amo", op="fetch_add", dtype="int64", pe=0, dest=a,
+                                    value=3)])[0]
+        t = srv.enqueue(req)
+        assert srv.wait(t) == 0
+        t0 = time.time()
+        with pytest.raises(B.B200Error) as e:
+            srv.wait(t + 5, timeout=0.05)
+        assert e.value.code == -6 and time.time() - t0 < 5.0
+        assert srv.poll(t + 5)[0] is False
+        assert srv.wait(srv.enqueue(req)) == 3
+    finally:
+        srv.stop()
+    assert B.get_rows(a, 8, np.int64, team=(0, 1, 1))[0, 0] == 6

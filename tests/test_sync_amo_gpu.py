@@ -115,3 +115,23 @@ def test_amo_bad_target_is_reported(B, heap):
     _, d_val = dev_array(B, heap, np.array([1], np.int64))
     with pytest.raises(B.B200Error):
         B.amo_batch("add", "int64", 1, d_pe, d_off, d_val)
+
+
+@pytest.mark.parametrize("algo", BARRIERS)
+def test_barrier_with_a_member_that_never_arrives_times_out_and_recovers(B, algo):
+    """Failure detection without a GPU fault: one member never arrives, every
+    wait that depends on it runs out of a 20 ms budget, the call returns
+    B200SHM_ERR_TIMEOUT, the flag lines are back at zero, and the same team's
+    next barrier completes."""
+    old = B.set_wait_budget(0.02)
+    try:
+        for team, absent in (((0, 1, 8), 5), ((3, 2, 17), 0), ((0, 1, 64), 63)):
+            with pytest.raises(B.B200Error) as e:
+                B.barrier_absent(algo, absent, team=team)
+            assert e.value.code == -6, e.value
+            assert B.barrier_flags_nonzero() == 0
+            B.barrier(algo, team=team)
+            assert B.barrier_flags_nonzero() == 0
+    finally:
+        B.set_wait_budget(old)
+    assert B.set_wait_budget(0) == pytest.approx(old)
