@@ -238,6 +238,8 @@ def main():
     ap.add_argument("--batch-reductions", type=int, default=4096)
     ap.add_argument("--batch-tune", default="off", choices=["auto", "off"],
                     help="batch workload: heuristic plan (off, the default) or the autotuner")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the config1/movement/batch/serve sub-objects of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -251,12 +253,12 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    if args.workload == "movement":
-        return run_movement(args, world, rank, local)
-    if args.workload == "batch":
-        return run_batch(args, world, rank, local)
-    if args.workload == "serve":
-        return run_serve(args, world, rank, local)
+    if args.workload != "reduce":
+        fn = {"movement": run_movement, "batch": run_batch, "serve": run_serve}[args.workload]
+        line = fn(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -389,6 +391,15 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    extras = {}
+    if world == 1 and not args.headline_only and not args.case and N == 1 << 20:
+        # the other configurations, each in its own arena, after the headline
+        B.finalize()
+        for name, fn in (("config1", run_config1), ("movement", run_movement),
+                         ("batch", run_batch), ("serve", run_serve)):
+            t0 = time.perf_counter()
+            extras[name] = fn(args, world, rank, local)
+            extras[name]["run_seconds"] = round(time.perf_counter() - t0, 1)
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -401,38 +412,164 @@ def main():
             "per_kernel_ms": {k: round(v[0], 4) for k, v in durs.items()},
             "per_kernel_gbs": {k: round(v[1] / (v[0] / 1e3) / 1e9, 1) for k, v in durs.items()},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    line.update(extras)
     print(json.dumps(line), flush=True)
+
+# ---------------------------------------------------------------------------
+# config 1: 8 PEs, int32 sum reduce + fcollect64 + barrier_all, latency
+# ---------------------------------------------------------------------------
+def run_config1(args, world, rank, local, reps=300):
+    """The reference's CPU-runnable configuration on the GPU: 8 PEs, team
+    WORLD, int32 sum_reduce of 1024 elements (rec_dbl, the default), then
+    fcollect64 of 256 int64 per PE, then barrier_all (binomial tree).  These
+    are latency-bound; reported in microseconds per call: blocking calls
+    through the C ABI (launch + synchronisation each, what an OpenSHMEM
+    call costs) and the three stream-ordered with one synchronisation; next
+    to the reference's own shcoll code over 8 emulated PEs on the host."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    import gen
+    import oracle
+    x, fc = gen.config1_inputs()
+    B.init(8, 4 << 20)
+    team = (0, 1, 8)
+    try:
+        src, dst = B.malloc(4096), B.malloc(4096)
+        fs, fd = B.malloc(2048), B.malloc(16384)
+        B.put_rows(src, x, team=team)
+        B.put_rows(fs, fc, team=team)
+        s_ptr = B.stream()
+
+        def red(stream=None):
+            B.reduce("sum", "int32", "rec_dbl", dst, src, 1024, team=team, stream=stream)
+
+        def fcol(stream=None):
+            B.fcollect(fd, fs, 2048, team=team, stream=stream)
+
+        def bar(stream=None):
+            B.barrier("binomial_tree", team=team, stream=stream)
+
+        def seq():
+            red(), fcol(), bar()
+
+        def seq_ordered():
+            red(s_ptr), fcol(s_ptr), bar(s_ptr)
+            B.quiet()
+
+        def med_us(fn):
+            for _ in range(20):
+                fn()
+            t = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                fn()
+                t.append(time.perf_counter() - t0)
+            return round(float(np.median(t)) * 1e6, 2)
+
+        gpu = {"int32_sum_reduce_us": med_us(red), "fcollect64_us": med_us(fcol),
+               "barrier_all_us": med_us(bar), "sequence_blocking_us": med_us(seq),
+               "sequence_stream_ordered_us": med_us(seq_ordered)}
+        red(), fcol()
+        z = np.load(os.path.join(ROOT, "tests", "golden", "config1.npz"))
+        exact = (B.get_rows(dst, 4096, np.int32, team=team).tobytes() == z["reduce_out"].tobytes()
+                 and B.get_rows(fd, 16384, np.int64, team=team).tobytes() ==
+                 z["fcollect_out"].tobytes())
+    finally:
+        B.finalize()
+    cpu = None
+    if oracle.Reference.available:
+        R = oracle.Reference()
+        out = np.zeros_like(x)
+        _, t_red = R.run(oracle.K_REDUCE_TEAM, "shcoll_int32_sum_reduce_rec_dbl", x, out,
+                         nelems=1024, warmup=20, iters=reps, pin=True)
+        out = np.zeros((8, 8 * 256), np.int64)
+        _, t_fc = R.run(oracle.K_SIZED, "shcoll_fcollect64_bruck_inplace", fc, out, nelems=256,
+                        warmup=20, iters=reps, pin=True)
+        _, t_bar = R.run(oracle.K_BARRIER_ALL, "shcoll_barrier_all_binomial_tree",
+                         np.zeros((8, 8), np.uint8), np.zeros((8, 8), np.uint8), warmup=20,
+                         iters=reps, pin=True)
+        m = [float(np.median(t)) * 1e6 for t in (t_red, t_fc, t_bar)]
+        cpu = {"int32_sum_reduce_us": round(m[0], 2), "fcollect64_us": round(m[1], 2),
+               "barrier_all_us": round(m[2], 2), "sequence_us": round(sum(m), 2),
+               "kind": "reference", "cores": 8,
+               "sample": "the reference's src/shcoll/src code (oracle/_ref) over 8 emulated PEs "
+                         "(pinned pthreads); median of %d calls between host barriers" % reps}
+    return {"workload": "config1: 8 PEs, int32 sum_reduce 1024 + fcollect64 256 + barrier_all",
+            "unit": "us per call (median of %d)" % reps, "gpu": gpu, "cpu_reference": cpu,
+            "bit_exact_vs_golden": bool(exact)}
+
 
 # ---------------------------------------------------------------------------
 # data movement (the 128-PE configuration)
 # ---------------------------------------------------------------------------
+def movement_cpu_reference():
+    """The reference's shcoll copies at the configuration's sizes over 128
+    emulated PEs, one timed call each (a bounded sample)."""
+    import gen
+    import oracle
+    if not oracle.Reference.available:
+        return None
+    R = oracle.Reference()
+    PM = 128
+    res = {}
+    x = gen.uniform_int(np.int64, PM, 4096, 33)
+    out = np.zeros((PM, PM * 4096), np.int64)
+    _, t = R.run(oracle.K_SIZED, "shcoll_fcollect64_bruck_inplace", x, out, nelems=4096, pin=True)
+    res["fcollect64"] = (PM * 4096 * 8 + PM * PM * 4096 * 8) / t[0] / 1e9
+    del x, out
+    x = gen.uniform_int(np.uint8, PM, PM * 65536, 31)
+    out = np.zeros_like(x)
+    _, t = R.run(oracle.K_TEAM_COPY, "shcoll_alltoallmem_shift_exchange_barrier", x, out,
+                 nelems=65536, pin=True)
+    res["alltoallmem"] = 2 * PM * PM * 65536 / t[0] / 1e9
+    del x, out
+    x = gen.uniform_int(np.int64, PM, PM * 4096 * 3, 32)
+    out = np.zeros((PM, PM * 4096 * 2), np.int64)
+    _, t = R.run(oracle.K_ALLTOALLS_SIZED, "shcoll_alltoalls64_shift_exchange_barrier", x, out,
+                 nelems=4096, a=2, b=3, pin=True)
+    res["alltoalls64"] = 2 * PM * PM * 4096 * 8 / t[0] / 1e9
+    return {"value": {k: round(v, 3) for k, v in res.items()}, "unit": "GB/s",
+            "cores": os.cpu_count() or 1, "kind": "reference",
+            "sample": "one call of each at the full size over 128 emulated PEs (pinned "
+                      "pthreads), the reference's src/shcoll/src code (oracle/_ref)"}
+
+
 def run_movement(args, world, rank, local):
     """128 emulated PEs: alltoallmem of 64 KiB per PE pair (uint8),
     alltoalls64 with dst stride 2 / src stride 3 over 4096 int64 per pair,
     fcollect64 of 4096 int64 per PE, and 2^20 int64 fetch-adds on 2^20
     counters per PE at uniformly random (PE, offset).  Each op is timed on
-    its own with CUDA events over --steps launches."""
+    its own with CUDA events over --steps launches, then its result is
+    checked bit for bit against the oracle."""
     import torch
     import __graft_entry__
     __graft_entry__.build_library()
     import b200shm as B
     import gen
+    import oracle
+    rs = oracle.Restatement()
     PM, BLK, NS, NF, NOPS, NCNT = 128, 64 << 10, 4096, 4096, 1 << 20, 1 << 20
     B.init(PM, 96 << 20)  # 12 GiB arena: 76 MiB of objects per PE
     team = (0, 1, PM)
     s_ptr = B.stream()
     st = torch.cuda.ExternalStream(s_ptr)
+    x_a2a = gen.uniform_int(np.uint8, PM, PM * BLK, 31)
+    x_as = gen.uniform_int(np.int64, PM, PM * NS * 3, 32)
+    x_fc = gen.uniform_int(np.int64, PM, NF, 33)
     a2a_s, a2a_d = B.malloc(PM * BLK), B.malloc(PM * BLK)
-    B.put_rows(a2a_s, gen.uniform_int(np.uint8, PM, PM * BLK, 31), team=team)
+    B.put_rows(a2a_s, x_a2a, team=team)
     as_s, as_d = B.malloc(PM * NS * 3 * 8), B.malloc(PM * NS * 2 * 8)
-    B.put_rows(as_s, gen.uniform_int(np.int64, PM, PM * NS * 3, 32), team=team)
+    B.put_rows(as_s, x_as, team=team)
+    B.memset(as_d, 0, PM * NS * 2 * 8, team=team)
     fc_s, fc_d = B.malloc(NF * 8), B.malloc(PM * NF * 8)
-    B.put_rows(fc_s, gen.uniform_int(np.int64, PM, NF, 33), team=team)
+    B.put_rows(fc_s, x_fc, team=team)
     cnt = B.malloc(NCNT * 8)
     B.memset(cnt, 0, NCNT * 8, team=team)
     rng = np.random.default_rng(34)
     pe = rng.integers(0, PM, NOPS).astype(np.int32)
-    off = (cnt + rng.integers(0, NCNT, NOPS) * 8).astype(np.uint64)
+    idx = rng.integers(0, NCNT, NOPS).astype(np.int64)
+    off = (cnt + idx * 8).astype(np.uint64)
     req = B.malloc(NOPS * (4 + 8 + 8 + 8) + 4096)  # request arrays live in PE 0's slice
     o_pe, o_off, o_val, o_f = req, req + NOPS * 4, req + NOPS * 12, req + NOPS * 20
     for o, arr in ((o_pe, pe), (o_off, off), (o_val, np.ones(NOPS, np.int64))):
@@ -440,19 +577,25 @@ def run_movement(args, world, rank, local):
     d = {k: B.ptr(0, o) for k, o in (("pe", o_pe), ("off", o_off), ("val", o_val), ("f", o_f))}
     ops = {
         "alltoallmem": (lambda: B.alltoall(a2a_d, a2a_s, BLK, team=team, stream=s_ptr),
-                        2 * PM * PM * BLK, "GB/s"),
+                        2 * PM * PM * BLK, "GB/s", "k_alltoall"),
         "alltoalls64": (lambda: B.alltoalls(as_d, as_s, 2, 3, NS, 8, team=team, stream=s_ptr),
-                        2 * PM * PM * NS * 8, "GB/s"),
+                        2 * PM * PM * NS * 8, "GB/s", "k_alltoalls"),
         "fcollect64": (lambda: B.fcollect(fc_d, fc_s, NF * 8, team=team, stream=s_ptr),
-                       PM * NF * 8 + PM * PM * NF * 8, "GB/s"),
+                       PM * NF * 8 + PM * PM * NF * 8, "GB/s", "k_fcollect"),
         "atomic_fetch_add": (lambda: B.amo_batch("fetch_add", "int64", NOPS, d["pe"], d["off"],
                                                  d["val"], None, d["f"], stream=s_ptr),
-                             NOPS, "Mops/s"),
+                             NOPS, "Mops/s", "k_amo"),
     }
     peak, peak_kind = peaks()
+    traffic = {}
+    tpath = os.path.join(ROOT, "profiles", "movement_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f)
     res = {}
     launches0 = B.launch_count()
-    for name, (fn, units, unit) in ops.items():
+    runs = args.warmup + args.steps
+    for name, (fn, units, unit, kern) in ops.items():
         for _ in range(args.warmup):
             fn()
         B.quiet()
@@ -464,16 +607,44 @@ def run_movement(args, world, rank, local):
         B.quiet()
         ms = e0.elapsed_time(e1) / args.steps
         rate = units / (ms / 1e3) / (1e9 if unit == "GB/s" else 1e6)
-        res[name] = {"ms": round(ms, 4), "value": round(rate, 1), "unit": unit}
+        res[name] = {"kernel": kern, "ms": round(ms, 4), "value": round(rate, 1), "unit": unit}
         if unit == "GB/s":
-            res[name]["frac_of_hbm"] = round(rate / peak, 4)
-    line = {"metric": METRIC, "workload": "movement", "n_gpus": world, "steps": args.steps,
+            res[name]["roofline"] = {"bound": "hbm", "achieved": round(rate, 1), "peak": peak,
+                                     "unit": "GB/s", "frac": round(rate / peak, 4),
+                                     "bytes_per_launch": units, "traffic": traffic.get(name)}
+        else:
+            res[name]["gbs_at_16B_per_op"] = round(units * 16 / (ms / 1e3) / 1e9, 1)
+            res[name]["traffic"] = traffic.get(name)
+    launches = B.launch_count() - launches0
+    # bit-exact checks of each op's last result against the oracle
+    got = B.get_rows(a2a_d, PM * BLK, np.uint8, team=team)
+    res["alltoallmem"]["bit_exact"] = got.tobytes() == rs.alltoall(x_a2a).tobytes()
+    del got
+    got = B.get_rows(as_d, PM * NS * 2 * 8, np.int64, team=team)
+    want = rs.alltoalls(x_as, np.zeros((PM, PM * NS * 2), np.int64), 2, 3, NS)
+    res["alltoalls64"]["bit_exact"] = got.tobytes() == want.tobytes()
+    del got, want
+    got = B.get_rows(fc_d, PM * NF * 8, np.int64, team=team)
+    res["fcollect64"]["bit_exact"] = got.tobytes() == rs.fcollect(x_fc).tobytes()
+    final = B.get_rows(cnt, NCNT * 8, np.int64, team=team)
+    fetched = B.get_rows(o_f, NOPS * 8, np.int64, team=(0, 1, 1))[0]
+    hist = np.bincount(pe.astype(np.int64) * NCNT + idx, minlength=PM * NCNT)
+    ok = np.array_equal(final.reshape(-1), runs * hist)
+    key = pe.astype(np.int64) * NCNT + idx  # the last run's fetches: a permutation per counter
+    order = np.lexsort((fetched, key))
+    ks, fs = key[order], fetched[order]
+    starts = np.r_[0, np.flatnonzero(np.diff(ks)) + 1]
+    rank_in = np.arange(NOPS) - np.repeat(starts, np.diff(np.r_[starts, NOPS]))
+    ok = ok and np.array_equal(fs, (runs - 1) * hist[ks] + rank_in)
+    res["atomic_fetch_add"]["bit_exact"] = bool(ok)
+    B.finalize()
+    cpu = movement_cpu_reference()
+    return {"workload": "movement", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "peak_gbs": peak, "peak_kind": peak_kind,
             "config": {"npes": PM, "alltoallmem_block": BLK, "alltoalls": "int64 dst=2 sst=3 n=4096",
-                       "fcollect64_nelems": NF, "amo": "2^20 fetch_add int64 on 2^20 counters/PE"},
-            "results": res, "gpu_launches": B.launch_count() - launches0}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+                       "fcollect64_nelems": NF, "amo": "2^20 fetch_add int64 on 2^20 counters/PE",
+                       "l2": "every copy moves >= 512 MiB (> L2); the AMO counters span 1 GiB"},
+            "results": res, "gpu_launches": launches, "cpu_baseline": cpu}
 
 
 # ---------------------------------------------------------------------------
@@ -612,8 +783,9 @@ def run_batch(args, world, rank, local):
             "speedup": round(pc_ms / b_ms, 2), "alg_bytes": total_bytes,
             "hbm_floor_ms": round(total_bytes / (peak * 1e9) * 1e3, 4), "peak_kind": peak_kind,
             "batch_matches_per_call": bool(match), "gpu_launches_per_batch": launches}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    batch.close()
+    B.finalize()
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -754,6 +926,8 @@ def run_serve(args, world, rank, local):
     pc_last = float(np.max(arrival[:npc] + lat_pc))
     lat_pc_sat, _ = B.replay(pc_reqs, np.zeros(npc))
     pc_sat_s = float(np.max(lat_pc_sat))
+    B.replay_ordered(pc_reqs[:min(npc, 2000)])  # warm-up
+    ord_s, _ = B.replay_ordered(pc_reqs)
     total_bytes = int(sum(it["bytes"] for it in items))
     line = {"metric": METRIC, "workload": "serve", "n_gpus": world,
             "config": {"npes": PS, "arena_gib": PS * SL / 2 ** 30, "teams": "64 x 4 PEs",
@@ -775,11 +949,17 @@ def run_serve(args, world, rank, local):
                          "ops_per_s": round(npc / pc_last, 1),
                          "saturated_ops_per_s": round(npc / pc_sat_s, 1),
                          "form": "one blocking b200shm_* call per request, in arrival order"},
+            "per_call_stream_ordered": {
+                "requests": npc, "ops_per_s": round(npc / ord_s, 1),
+                "form": "the same per-call entry points issued back to back on one stream, "
+                        "one synchronisation at the end (b200shm_serve_replay_ordered)"},
             "amo_fetch_adds": int(sum(1 for it in items if it["kind"] == "amo"))}
     line["speedup_saturated_ops"] = round(line["served"]["saturated_ops_per_s"] /
                                           line["per_call"]["saturated_ops_per_s"], 2)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    line["speedup_saturated_ops_vs_stream_ordered"] = round(
+        line["served"]["saturated_ops_per_s"] / line["per_call_stream_ordered"]["ops_per_s"], 2)
+    B.finalize()
+    return line
 
 
 if __name__ == "__main__":

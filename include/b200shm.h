@@ -83,6 +83,28 @@ int b200shm_get_host(void *host_dst, int pe_start, int pe_stride, int pe_count,
  * or host memory); blocking when stream is NULL.  Backs shmem_putmem /
  * shmem_getmem (src/shmemc/ucx/comms.c:677-737). */
 int b200shm_memcpy(void *dst, const void *src, uint64_t bytes, void *stream);
+/* Strided copy of nelems elements of elem_bytes: dst[i*dst_stride] =
+ * src[i*src_stride] (strides in elements, >= 1), between any memory the
+ * device can see; blocking when stream is NULL.  Backs shmem_<T>_iput /
+ * iget and shmem_iput/iget{8,16,32,64,128} (src/api/rma/putget.h:131-220,
+ * which issue one UCX put or get per element). */
+int b200shm_memcpy_strided(void *dst, int64_t dst_stride, const void *src, int64_t src_stride,
+                           uint64_t elem_bytes, uint64_t nelems, void *stream);
+/* Compare nelems symmetric words of `dtype` (a 2-, 4- or 8-byte integer
+ * type, compared as that type) at offset `off` of PE `pe` with cmp
+ * (SHMEM_CMP_EQ/NE/GT/LE/LT/GE = 0..5) against *cmp_value, or against
+ * cmp_values[i] when cmp_values is not NULL (host arrays of the element
+ * type).  out[i] (host) receives 1 when element i compares true, 0 when
+ * not, 2 when status (may be NULL) is non-zero at i; loaded (may be NULL)
+ * receives the bits each element held when it was compared.  One device
+ * pass with acquire loads, so words written by the engine's puts, atomics
+ * and serving loop are seen.  Blocking.  Backs shmem_<T>_test,
+ * test_all/any/some[_vector], and in a polling loop wait_until,
+ * wait_until_all/any/some[_vector] and shmem_signal_wait_until
+ * (src/shmemc/ucx/test.c:10-170, waituntil.c:18-320). */
+int b200shm_test_words(int cmp, int dtype, int pe, uint64_t off, uint64_t nelems,
+                       const int *status, const void *cmp_value, const void *cmp_values,
+                       uint8_t *out, uint64_t *loaded);
 /* Fill bytes_per_pe bytes at `off` of pe_count members with `byte`. */
 int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off,
                    int byte, uint64_t bytes_per_pe, void *stream);
@@ -280,7 +302,15 @@ enum b200shm_req_kind {
 /* One request.  REDUCE: op/dtype/algo/team/dest/src/n = nelems, as
  * b200shm_reduce (dtype one of I32, U32, I64, U64, F32, F64).  AMO: op is
  * a b200shm_amo, dtype a 4- or 8-byte type, value/cond hold the operand
- * bits, the old value comes back through b200shm_serve_poll. */
+ * bits, the old value comes back through b200shm_serve_poll.  Any other
+ * kind may pass dest_off = B200SHM_SERVE_ALLOC: the loop then allocates the
+ * dest from the symmetric heap (the bytes one member's dest spans) when it
+ * admits the request, so the request waits in the ring, in arrival order,
+ * until the heap has room; b200shm_serve_poll / _wait return the offset it
+ * got, and the caller releases it with b200shm_free.  A request waiting for
+ * room keeps the loop awake, and b200shm_serve_stop waits (bounded) for it
+ * to be admitted.  The per-call replays take no such request. */
+#define B200SHM_SERVE_ALLOC (~(uint64_t)0)
 typedef struct b200shm_request {
   int32_t kind, op, dtype, algo;
   int32_t pe_start, pe_stride, pe_size, pe;
@@ -299,7 +329,7 @@ typedef struct b200shm_server b200shm_server;
  * no new request has arrived for idle_seconds (0 = 0.25 s) the CTAs exit;
  * the next enqueue, poll or wait relaunches the kernel, so the loop holds
  * the GPU only while it is used.  Replaces the reference's issue-one-call-and-wait model
- * (shmem_* -> shcoll / shmemc_ctx_* round trips, src/shcoll/src/*.c,
+ * (shmem_* -> shcoll / shmemc_ctx_* round trips, src/shcoll/src/ files,
  * src/shmemc/ucx/comms.c) for streams of small operations.  Requests in
  * flight together may run in any order and concurrently, as non-blocking
  * (_nbi) operations do: a request that depends on another's result must
@@ -328,8 +358,10 @@ int b200shm_serve_start_budget(uint32_t queue_slots, int ctas, double idle_secon
  * B200SHM_ERR_BUSY when all queue slots hold requests not yet complete. */
 int b200shm_serve_enqueue(b200shm_server *srv, const b200shm_request *req,
                           uint64_t *ticket);
-/* 1 when the request completed (its AMO old value in *fetched, which may
- * be NULL), 0 while it is pending, < 0 on an error. */
+/* 1 when the request completed, 0 while it is pending, < 0 on an error.
+ * *fetched (may be NULL) receives an AMO's old value, and for the other
+ * kinds the dest offset the request wrote to (the one the loop allocated,
+ * for B200SHM_SERVE_ALLOC). */
 int b200shm_serve_poll(b200shm_server *srv, uint64_t ticket, uint64_t *fetched);
 /* Device clock stamps (globaltimer, ns) of a completed request still in
  * its slot: copied from the ring into device memory, its last tiles
@@ -350,6 +382,17 @@ int b200shm_serve_stop(b200shm_server *srv);
  * benchmark and its per-call comparison. */
 int b200shm_serve_replay(b200shm_server *srv, const b200shm_request *reqs, uint64_t n,
                          const double *arrival_s, double *latency_s, uint64_t *fetched);
+/* The per-call comparison in stream order: every request through its
+ * per-call entry point on `stream` (NULL = the library stream) with no
+ * synchronisation between requests -- b200shm_reduce, _fcollect,
+ * _alltoall, a device copy for put/get, one single-operation atomic kernel
+ * -- then one synchronisation.  *seconds (may be NULL) receives the time
+ * from the first issue to the last completion, fetched (may be NULL) the
+ * AMO old values.  Requests must not depend on each other's results (they
+ * complete in stream order).  The reference has no stream-ordered form: a
+ * measuring tool for the serving benchmark. */
+int b200shm_serve_replay_ordered(const b200shm_request *reqs, uint64_t n, void *stream,
+                                 double *seconds, uint64_t *fetched);
 
 /* Fill nelems elements of `dtype` at `off` in pe_count members with seeded
  * pseudo-random values: integers uniform in [lo, hi], floats uniform in

@@ -9,8 +9,12 @@
  * barrier_all/sync_all/barrier/sync/team_sync, the reductions
  * (shmem_<T>_<op>_reduce and shmem_<T>_<op>_to_all over the reference's type
  * tables), fcollect / collect / broadcast / alltoall / alltoalls in their typed, mem
- * and 32/64 forms, the atomics (shmem_[ctx_]<T>_atomic_*), and teams
- * (world, split_strided, split_2d, my_pe, n_pes, translate, destroy).
+ * and 32/64 forms, the atomics (shmem_[ctx_]<T>_atomic_*), teams
+ * (world, split_strided, split_2d, my_pe, n_pes, translate, destroy), the
+ * strided and signalled puts and gets (iput/iget, put_signal[_nbi], the
+ * sized put/get forms) and the point-to-point waits and tests
+ * (wait_until / test and their _all/_any/_some[_vector] forms,
+ * signal_fetch / signal_wait_until).
  *
  * How PEs run: every PE is a host thread of one process, started by
  * shmemx_b200_run (include/shmemx.h); its symmetric heap is a slice of one
@@ -368,6 +372,148 @@ SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_NBI_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_NBI_BIT)
+
+/* ---- strided and signalled RMA (api.h:355-600, 714-1000) ----------------
+ * iput/iget: dest[i*tst] = source[i*sst] for i < nelems (strides in
+ * elements, >= 1), one side symmetric on `pe`.  put_signal: the data is
+ * delivered, then *sig_addr on `pe` is set to or increased by `signal`
+ * (sig_op SHMEM_SIGNAL_SET / SHMEM_SIGNAL_ADD); the _nbi forms complete
+ * before they return. */
+enum { SHMEM_SIGNAL_SET = 0, SHMEM_SIGNAL_ADD };
+#define SHMEM_B200_DECL_RMA_STRIDED(_type, _tn)                                 \
+  void shmem_##_tn##_iput(_type *dest, const _type *source, ptrdiff_t tst,     \
+                          ptrdiff_t sst, size_t nelems, int pe);                \
+  void shmem_##_tn##_iget(_type *dest, const _type *source, ptrdiff_t tst,     \
+                          ptrdiff_t sst, size_t nelems, int pe);                \
+  void shmem_ctx_##_tn##_iput(shmem_ctx_t ctx, _type *dest,                    \
+                              const _type *source, ptrdiff_t tst,               \
+                              ptrdiff_t sst, size_t nelems, int pe);            \
+  void shmem_ctx_##_tn##_iget(shmem_ctx_t ctx, _type *dest,                    \
+                              const _type *source, ptrdiff_t tst,               \
+                              ptrdiff_t sst, size_t nelems, int pe);            \
+  void shmem_##_tn##_put_signal(_type *dest, const _type *source,              \
+                                size_t nelems, uint64_t *sig_addr,              \
+                                uint64_t signal, int sig_op, int pe);           \
+  void shmem_##_tn##_put_signal_nbi(_type *dest, const _type *source,          \
+                                    size_t nelems, uint64_t *sig_addr,          \
+                                    uint64_t signal, int sig_op, int pe);       \
+  void shmem_ctx_##_tn##_put_signal(shmem_ctx_t ctx, _type *dest,              \
+                                    const _type *source, size_t nelems,         \
+                                    uint64_t *sig_addr, uint64_t signal,        \
+                                    int sig_op, int pe);                        \
+  void shmem_ctx_##_tn##_put_signal_nbi(shmem_ctx_t ctx, _type *dest,          \
+                                        const _type *source, size_t nelems,     \
+                                        uint64_t *sig_addr, uint64_t signal,    \
+                                        int sig_op, int pe);
+SHMEM_B200_RMA_TYPES(SHMEM_B200_DECL_RMA_STRIDED)
+#define SHMEM_B200_DECL_RMA_SIZED(_bits)                                        \
+  void shmem_put##_bits(void *dest, const void *source, size_t nelems, int pe); \
+  void shmem_get##_bits(void *dest, const void *source, size_t nelems, int pe); \
+  void shmem_put##_bits##_nbi(void *dest, const void *source, size_t nelems,   \
+                              int pe);                                          \
+  void shmem_get##_bits##_nbi(void *dest, const void *source, size_t nelems,   \
+                              int pe);                                          \
+  void shmem_iput##_bits(void *dest, const void *source, ptrdiff_t tst,        \
+                         ptrdiff_t sst, size_t nelems, int pe);                 \
+  void shmem_iget##_bits(void *dest, const void *source, ptrdiff_t tst,        \
+                         ptrdiff_t sst, size_t nelems, int pe);                 \
+  void shmem_ctx_put##_bits(shmem_ctx_t ctx, void *dest, const void *source,   \
+                            size_t nelems, int pe);                             \
+  void shmem_ctx_get##_bits(shmem_ctx_t ctx, void *dest, const void *source,   \
+                            size_t nelems, int pe);                             \
+  void shmem_ctx_put##_bits##_nbi(shmem_ctx_t ctx, void *dest,                 \
+                                  const void *source, size_t nelems, int pe);   \
+  void shmem_ctx_get##_bits##_nbi(shmem_ctx_t ctx, void *dest,                 \
+                                  const void *source, size_t nelems, int pe);   \
+  void shmem_ctx_iput##_bits(shmem_ctx_t ctx, void *dest, const void *source,  \
+                             ptrdiff_t tst, ptrdiff_t sst, size_t nelems,       \
+                             int pe);                                           \
+  void shmem_ctx_iget##_bits(shmem_ctx_t ctx, void *dest, const void *source,  \
+                             ptrdiff_t tst, ptrdiff_t sst, size_t nelems,       \
+                             int pe);                                           \
+  void shmem_put##_bits##_signal(void *dest, const void *source,               \
+                                 size_t nelems, uint64_t *sig_addr,             \
+                                 uint64_t signal, int sig_op, int pe);          \
+  void shmem_put##_bits##_signal_nbi(void *dest, const void *source,           \
+                                     size_t nelems, uint64_t *sig_addr,         \
+                                     uint64_t signal, int sig_op, int pe);      \
+  void shmem_ctx_put##_bits##_signal(shmem_ctx_t ctx, void *dest,              \
+                                     const void *source, size_t nelems,         \
+                                     uint64_t *sig_addr, uint64_t signal,       \
+                                     int sig_op, int pe);                       \
+  void shmem_ctx_put##_bits##_signal_nbi(shmem_ctx_t ctx, void *dest,          \
+                                         const void *source, size_t nelems,     \
+                                         uint64_t *sig_addr, uint64_t signal,   \
+                                         int sig_op, int pe);
+SHMEM_B200_DECL_RMA_SIZED(8)
+SHMEM_B200_DECL_RMA_SIZED(16)
+SHMEM_B200_DECL_RMA_SIZED(32)
+SHMEM_B200_DECL_RMA_SIZED(64)
+SHMEM_B200_DECL_RMA_SIZED(128)
+void shmem_putmem_signal(void *dest, const void *source, size_t nelems, uint64_t *sig_addr,
+                         uint64_t signal, int sig_op, int pe);
+void shmem_putmem_signal_nbi(void *dest, const void *source, size_t nelems, uint64_t *sig_addr,
+                             uint64_t signal, int sig_op, int pe);
+void shmem_ctx_putmem_signal(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                             uint64_t *sig_addr, uint64_t signal, int sig_op, int pe);
+void shmem_ctx_putmem_signal_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                                 uint64_t *sig_addr, uint64_t signal, int sig_op, int pe);
+/* the signal word of the calling PE (api.h:1004-1046) */
+uint64_t shmem_signal_fetch(const uint64_t *sig_addr);
+uint64_t shmem_signal_wait_until(uint64_t *sig_addr, int cmp, uint64_t cmp_value);
+
+/* ---- point-to-point synchronisation (api.h:1472-2015) --------------------
+ * On symmetric variables of the calling PE, compared as their own type.
+ * status (may be NULL) excludes element i when status[i] != 0.  test_any
+ * and wait_until_any return the lowest index that compares true (SIZE_MAX
+ * when there is none, or every element is excluded); test_some and
+ * wait_until_some write the indices that compare true and return their
+ * count.  The waits block until the condition holds; SHMEM_B200_WAIT_TIMEOUT
+ * (seconds) bounds them (then shmemx_b200_last_status() is
+ * B200SHM_ERR_TIMEOUT). */
+#define SHMEM_B200_SYNC_TYPES(X)                                                \
+  X(short, short) X(unsigned short, ushort) SHMEM_B200_AMO_STANDARD_TYPES(X)
+#define SHMEM_B200_DECL_SYNC_ONE(_type, _tn)                                    \
+  int shmem_##_tn##_test(_type *ivar, int cmp, _type cmp_value);               \
+  void shmem_##_tn##_wait_until(_type *ivar, int cmp, _type cmp_value);        \
+  void shmem_##_tn##_wait(_type *ivar, _type cmp_value);
+#define SHMEM_B200_DECL_SYNC_VEC(_type, _tn)                                    \
+  int shmem_##_tn##_test_all(_type *ivars, size_t nelems, const int *status,   \
+                             int cmp, _type cmp_value);                         \
+  size_t shmem_##_tn##_test_any(_type *ivars, size_t nelems,                   \
+                                const int *status, int cmp, _type cmp_value);   \
+  size_t shmem_##_tn##_test_some(_type *ivars, size_t nelems, size_t *indices, \
+                                 const int *status, int cmp, _type cmp_value);  \
+  int shmem_##_tn##_test_all_vector(_type *ivars, size_t nelems,               \
+                                    const int *status, int cmp,                 \
+                                    _type *cmp_values);                         \
+  size_t shmem_##_tn##_test_any_vector(_type *ivars, size_t nelems,            \
+                                       const int *status, int cmp,              \
+                                       _type *cmp_values);                      \
+  size_t shmem_##_tn##_test_some_vector(_type *ivars, size_t nelems,           \
+                                        size_t *indices, const int *status,     \
+                                        int cmp, _type *cmp_values);            \
+  void shmem_##_tn##_wait_until_all(_type *ivars, size_t nelems,               \
+                                    const int *status, int cmp,                 \
+                                    _type cmp_value);                           \
+  size_t shmem_##_tn##_wait_until_any(_type *ivars, size_t nelems,             \
+                                      const int *status, int cmp,               \
+                                      _type cmp_value);                         \
+  size_t shmem_##_tn##_wait_until_some(_type *ivars, size_t nelems,            \
+                                       size_t *indices, const int *status,      \
+                                       int cmp, _type cmp_value);               \
+  void shmem_##_tn##_wait_until_all_vector(_type *ivars, size_t nelems,        \
+                                           const int *status, int cmp,          \
+                                           _type *cmp_values);                  \
+  size_t shmem_##_tn##_wait_until_any_vector(_type *ivars, size_t nelems,      \
+                                             const int *status, int cmp,        \
+                                             _type *cmp_values);                \
+  size_t shmem_##_tn##_wait_until_some_vector(_type *ivars, size_t nelems,     \
+                                              size_t *indices,                  \
+                                              const int *status, int cmp,       \
+                                              _type *cmp_values);
+SHMEM_B200_SYNC_TYPES(SHMEM_B200_DECL_SYNC_ONE)
+SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_SYNC_VEC)
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ ALGOS = ["linear", "binomial", "rec_dbl", "rabenseifner", "rabenseifner2"]
 BARRIER_ALGOS = ["linear", "complete_tree", "binomial_tree", "knomial_tree", "dissemination"]
 AMOS = ["fetch_add", "add", "fetch_inc", "inc", "swap", "cswap", "set", "fetch", "fetch_and",
         "and", "fetch_or", "or", "fetch_xor", "xor"]
+SERVE_ALLOC = (1 << 64) - 1  # request dest_off: the serving loop allocates the dest
 STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_UNSUPPORTED", -3: "ERR_NOMEM", -4: "ERR_CUDA",
           -5: "ERR_STATE", -6: "ERR_TIMEOUT", -7: "ERR_BUSY"}
 
@@ -88,6 +89,7 @@ def _load():
         "b200shm_serve_stop": (ci, [vp]),
         "b200shm_serve_trace": (ci, [vp, u64, vp]),
         "b200shm_serve_replay": (ci, [vp, vp, u64, vp, vp, vp]),
+        "b200shm_serve_replay_ordered": (ci, [vp, u64, vp, ctypes.POINTER(ctypes.c_double), vp]),
         "b200shm_amo": (ci, [ci, ci, ci, u64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -424,3 +426,14 @@ def replay(reqs, arrival_s, server=None):
     _check(lib.b200shm_serve_replay(server.h if server else None, ctypes.cast(reqs, ctypes.c_void_p),
                                     n, arr.ctypes.data, lat.ctypes.data, fet.ctypes.data))
     return lat, fet
+
+
+def replay_ordered(reqs, stream=None):
+    """Every request through its per-call entry point, stream-ordered, one
+    synchronisation at the end: returns (seconds, fetched values)."""
+    n = len(reqs)
+    fet = np.zeros(n, np.uint64)
+    sec = ctypes.c_double()
+    _check(lib.b200shm_serve_replay_ordered(ctypes.cast(reqs, ctypes.c_void_p), n, stream,
+                                            ctypes.byref(sec), fet.ctypes.data))
+    return sec.value, fet

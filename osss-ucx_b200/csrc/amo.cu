@@ -85,6 +85,31 @@ int amo_launch(int amo, int dtype, uint64_t nops, const int32_t *pe, const uint6
   return B200SHM_OK;
 }
 
+/* One operation with its operands by value (the low 4 or 8 bytes of
+ * value/cond), stream-ordered; the old value goes to `fetched` (a device or
+ * mapped-host word, may be NULL).  The target is checked on the host. */
+int amo_one_launch(int amo, int dtype, int pe, uint64_t off, uint64_t value, uint64_t cond,
+                   void *fetched, cudaStream_t s) {
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (amo < 0 || amo >= B200SHM_AMO_NOP) return fail(B200SHM_ERR_ARG, "amo: unknown op %d", amo);
+  const bool w4 = dtype == B200SHM_I32 || dtype == B200SHM_U32 || dtype == B200SHM_F32;
+  const bool w8 = dtype == B200SHM_I64 || dtype == B200SHM_U64 || dtype == B200SHM_F64;
+  if (!w4 && !w8) return fail(B200SHM_ERR_UNSUPPORTED, "amo: dtype %d is not 4 or 8 bytes", dtype);
+  const uint64_t w = w8 ? 8 : 4;
+  if (pe < 0 || pe >= st().npes || off > st().slice - w || off % w)
+    return fail(B200SHM_ERR_ARG, "amo: target (PE %d, offset %llu) is not a %llu-byte word of the heap",
+                pe, (unsigned long long)off, (unsigned long long)w);
+  char *target = st().base + (uint64_t)pe * st().slice + off;
+  if (w8)
+    k_amo_one<unsigned long long><<<1, 1, 0, s>>>(amo, (unsigned long long *)target, value, cond,
+                                                  (unsigned long long *)fetched, 1);
+  else
+    k_amo_one<unsigned int><<<1, 1, 0, s>>>(amo, (unsigned int *)target, (unsigned int)value,
+                                            (unsigned int)cond, (unsigned int *)fetched, 1);
+  count_launch();
+  return B200SHM_OK;
+}
+
 }  // namespace b200
 
 extern "C" int b200shm_amo_batch(int amo, int dtype, uint64_t nops, const int32_t *pe,

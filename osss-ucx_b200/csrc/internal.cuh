@@ -100,6 +100,18 @@ inline unsigned grid_for(uint64_t items, int threads, int per_sm) {
 int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int pe_size,
                   uint64_t dest_off, uint64_t src_off, uint64_t nelems, cudaStream_t s);
 
+/* The device allocator of the symmetric heap (heap.cu, heap_core.cuh). */
+int heap_setup(uint64_t slice);
+void heap_teardown();
+int heap_alloc(uint64_t bytes, uint64_t align, uint64_t *off);
+int heap_release(uint64_t off);
+uint64_t heap_free_bytes();
+unsigned heap_unit_shift();
+
+/* One atomic with operands by value, stream-ordered (amo.cu). */
+int amo_one_launch(int amo, int dtype, int pe, uint64_t off, uint64_t value, uint64_t cond,
+                   void *fetched, cudaStream_t s);
+
 /* Member addressing: member i of a team lives at
  * base + (pe_start + i*pe_stride) * slice + off. */
 struct Members {

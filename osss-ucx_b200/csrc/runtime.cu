@@ -1,21 +1,21 @@
 /*
- * runtime.cu -- arena, symmetric allocator, host<->heap copies and error
- * handling of the B200 engine.
+ * runtime.cu -- arena, host<->heap copies and error handling of the B200
+ * engine.
  *
  * The reference gives every PE (an OS process) its own heap registered
  * with UCX (src/shmemc/ucx/init.c:174-218) and a dlmalloc mspace on top
  * (src/api/allocator/memalloc.c).  Here all PEs share one HBM arena: PE p
- * owns slice p, and symmetric allocation is a single first-fit allocator
- * over slice offsets, which is symmetric by construction (the reference
- * gets symmetry by having every PE allocate in the same order, with a
- * barrier in shmem_malloc, src/api/shmalloc.c:47-61).
+ * owns slice p, and symmetric allocation is one allocator over slice
+ * offsets, which is symmetric by construction (the reference gets symmetry
+ * by having every PE allocate in the same order, with a barrier in
+ * shmem_malloc, src/api/shmalloc.c:47-61).  The allocator runs on the
+ * device (heap_core.cuh, heap.cu).
  */
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <atomic>
-#include <map>
 #include <mutex>
 
 #include "internal.cuh"
@@ -107,18 +107,6 @@ int check_extent(uint64_t off, uint64_t bytes, const char *what) {
   return B200SHM_OK;
 }
 
-/* ---- symmetric allocator ------------------------------------------------ */
-static std::mutex g_heap_mu;
-static std::map<uint64_t, uint64_t> g_free;  /* offset -> size */
-static std::map<uint64_t, uint64_t> g_used;  /* offset -> size */
-
-static void heap_reset(uint64_t slice) {
-  std::lock_guard<std::mutex> lk(g_heap_mu);
-  g_free.clear();
-  g_used.clear();
-  g_free[0] = slice;
-}
-
 }  // namespace b200
 
 using namespace b200;
@@ -182,8 +170,18 @@ int b200shm_init(int npes, uint64_t heap_bytes_per_pe, int flags) {
   }
   s.npes = npes;
   s.slice = slice;
+  const int hrc = heap_setup(slice); /* the allocator's state, on the device */
+  if (hrc != B200SHM_OK) {
+    cudaStreamDestroy(s.stream);
+    cudaFree(s.base);
+    cudaFree(s.flags);
+    cudaFreeHost(s.h_status);
+    cudaFree(s.fix_list);
+    cudaFree(s.fix_count);
+    s = State();
+    return hrc;
+  }
   s.up = true;
-  heap_reset(slice);
   return B200SHM_OK;
 }
 
@@ -197,8 +195,8 @@ int b200shm_finalize(void) {
   cudaFreeHost(s.h_status);
   cudaFree(s.fix_list);
   cudaFree(s.fix_count);
+  heap_teardown();
   s = State();
-  heap_reset(0);
   return B200SHM_OK;
 }
 
@@ -220,56 +218,17 @@ int b200shm_malloc(uint64_t bytes, uint64_t align, uint64_t *off) {
   if (align < 256) align = 256; /* keeps every object 128-bit and TMA aligned */
   if (align & (align - 1)) return fail(B200SHM_ERR_ARG, "alignment %llu is not a power of two",
                                        (unsigned long long)align);
-  if (bytes == 0) bytes = 1;
-  bytes = (bytes + 255) & ~255ull;
-  std::lock_guard<std::mutex> lk(g_heap_mu);
-  for (auto it = g_free.begin(); it != g_free.end(); ++it) {
-    const uint64_t start = it->first, size = it->second;
-    const uint64_t a = (start + align - 1) & ~(align - 1);
-    if (a + bytes > start + size) continue;
-    g_free.erase(it);
-    if (a > start) g_free[start] = a - start;
-    if (start + size > a + bytes) g_free[a + bytes] = start + size - (a + bytes);
-    g_used[a] = bytes;
-    *off = a;
-    return B200SHM_OK;
-  }
-  return fail(B200SHM_ERR_NOMEM, "symmetric heap exhausted (%llu bytes requested)",
-              (unsigned long long)bytes);
+  if (bytes > st().slice) return fail(B200SHM_ERR_NOMEM, "symmetric heap exhausted (%llu bytes requested)",
+                                      (unsigned long long)bytes);
+  return heap_alloc(bytes, align, off);
 }
 
 int b200shm_free(uint64_t off) {
-  std::lock_guard<std::mutex> lk(g_heap_mu);
-  auto it = g_used.find(off);
-  if (it == g_used.end())
-    return fail(B200SHM_ERR_ARG, "offset %llu is not an allocated symmetric object",
-                (unsigned long long)off);
-  uint64_t start = off, size = it->second;
-  g_used.erase(it);
-  auto nx = g_free.lower_bound(start);
-  if (nx != g_free.end() && start + size == nx->first) {
-    size += nx->second;
-    g_free.erase(nx);
-  }
-  auto pv = g_free.lower_bound(start);
-  if (pv != g_free.begin()) {
-    --pv;
-    if (pv->first + pv->second == start) {
-      start = pv->first;
-      size += pv->second;
-      g_free.erase(pv);
-    }
-  }
-  g_free[start] = size;
-  return B200SHM_OK;
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  return heap_release(off);
 }
 
-uint64_t b200shm_heap_free_bytes(void) {
-  std::lock_guard<std::mutex> lk(g_heap_mu);
-  uint64_t t = 0;
-  for (auto &kv : g_free) t += kv.second;
-  return t;
-}
+uint64_t b200shm_heap_free_bytes(void) { return st().up ? heap_free_bytes() : 0; }
 
 /* One 2-D copy moves all members' rows when the member pitch fits the
  * copy engine's pitch limit; otherwise one copy per member. */
@@ -319,6 +278,26 @@ int b200shm_memcpy(void *dst, const void *src, uint64_t bytes, void *stream) {
   if (!dst || !src) return fail(B200SHM_ERR_ARG, "memcpy: null pointer");
   B200_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, pick_stream(stream)));
   return finish(stream, "b200shm_memcpy");
+}
+
+int b200shm_memcpy_strided(void *dst, int64_t dst_stride, const void *src, int64_t src_stride,
+                           uint64_t elem_bytes, uint64_t nelems, void *stream) {
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (nelems == 0 || elem_bytes == 0) return B200SHM_OK;
+  if (!dst || !src) return fail(B200SHM_ERR_ARG, "memcpy_strided: null pointer");
+  if (dst_stride < 1 || src_stride < 1)
+    return fail(B200SHM_ERR_ARG, "memcpy_strided: strides must be positive");
+  const uint64_t dp = (uint64_t)dst_stride * elem_bytes, sp = (uint64_t)src_stride * elem_bytes;
+  if (dp / elem_bytes != (uint64_t)dst_stride || sp / elem_bytes != (uint64_t)src_stride)
+    return fail(B200SHM_ERR_ARG, "memcpy_strided: stride overflows");
+  cudaStream_t s = pick_stream(stream);
+  if (dp == elem_bytes && sp == elem_bytes) {
+    B200_CK(cudaMemcpyAsync(dst, src, elem_bytes * nelems, cudaMemcpyDefault, s));
+  } else {
+    /* one 2-D copy: a row per element, the strides as pitches */
+    B200_CK(cudaMemcpy2DAsync(dst, dp, src, sp, elem_bytes, nelems, cudaMemcpyDefault, s));
+  }
+  return finish(stream, "b200shm_memcpy_strided");
 }
 
 int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off, int byte,

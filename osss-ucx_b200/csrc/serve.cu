@@ -48,6 +48,7 @@
 #include <vector>
 
 #include "amo_core.cuh"
+#include "heap_core.cuh"
 #include "internal.cuh"
 #include "reduce_core.cuh"
 
@@ -80,6 +81,20 @@ __host__ __device__ __forceinline__ unsigned long long heap_bytes(const b200shm_
   case B200SHM_REQ_PUT:
   case B200SHM_REQ_GET: return r.n;
   default: return 8;
+  }
+}
+/* The bytes one member's dest spans: what the loop allocates for a request
+ * whose dest_off is B200SHM_SERVE_ALLOC. */
+__host__ __device__ __forceinline__ unsigned long long dest_bytes(const b200shm_request &r) {
+  const unsigned long long P = r.pe_size > 0 ? (unsigned long long)r.pe_size : 1ull;
+  switch (r.kind) {
+  case B200SHM_REQ_REDUCE: {
+    const bool w8 = r.dtype == B200SHM_I64 || r.dtype == B200SHM_U64 || r.dtype == B200SHM_F64;
+    return r.n * (w8 ? 8ull : 4ull);
+  }
+  case B200SHM_REQ_FCOLLECT:
+  case B200SHM_REQ_ALLTOALL: return r.n * P;
+  default: return r.n;
   }
 }
 constexpr unsigned kMirrorMax = 1024; /* the largest mirror batch */
@@ -185,6 +200,7 @@ struct SArgs {
   unsigned long long epoch; /* this launch's number, reported in ctl->down */
   unsigned mirror_batch;    /* requests one poll copies at most */
   unsigned long long budget; /* heap bytes admitted requests may hold, 0 = no limit */
+  HeapDev heap;              /* the symmetric-heap allocator, for B200SHM_SERVE_ALLOC dests */
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long *p) {
@@ -610,10 +626,12 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
   unsigned n = (unsigned)(upto - from);
   __shared__ unsigned long long s_bytes[kMirrorMax]; /* heap bytes per request (budget only) */
   __shared__ unsigned long long s_nt[kMirrorMax];    /* tiles per request, as copied */
-  __shared__ unsigned s_admit;
+  __shared__ unsigned char s_alloc[kMirrorMax];      /* the loop allocates the dest */
+  __shared__ unsigned s_admit, s_nalloc;
   /* a snapshot taken early, overlapping the copy: completions only lower
    * the count meanwhile, so an early reading can only admit less */
   const unsigned long long used = a.budget && threadIdx.x == 0 ? vld(&a.dev->inflight) : 0;
+  if (threadIdx.x == 0) s_nalloc = 0;
   for (unsigned i = threadIdx.x; i < n; i += kServeThreads)
     ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[14] = 0;
   fence_gpu();
@@ -638,21 +656,42 @@ __device__ void mirror_ring(const SArgs &a, unsigned long long from, unsigned lo
         ((volatile unsigned long long *)&a.mreq[(from + i) % a.Q])[k] = k == 15 ? now : v[j];
       if (w < n * 16 && k == 15) s_bytes[i] = v[j];
       if (w < n * 16 && k == 9) s_nt[i] = v[j];
+      if (w < n * 16 && k == 4) { /* the dest offset */
+        s_alloc[i] = v[j] == B200SHM_SERVE_ALLOC;
+        if (v[j] == B200SHM_SERVE_ALLOC) atomicAdd(&s_nalloc, 1u);
+      }
     }
   }
   fence_gpu();
   __syncthreads();
-  if (a.budget) {
-    /* admission by heap bytes: the longest run of the batch, in arrival
-     * order, whose bytes fit beside those of the admitted requests not yet
-     * complete.  Only the poll-lock holder adds to the count and completions
-     * only lower it, so the check cannot overshoot.  The rest stay in the
-     * host ring for a later poll. */
+  if (a.budget || s_nalloc) {
+    /* admission: the longest run of the batch, in arrival order, whose
+     * bytes fit beside those of the admitted requests not yet complete
+     * (with a budget), and whose dests the heap can hold (for requests
+     * that ask the loop to allocate theirs).  Only the poll-lock holder
+     * adds to the count and completions only lower it, so the check cannot
+     * overshoot.  The rest stay in the host ring for a later poll. */
     if (threadIdx.x == 0) {
       unsigned long long add = 0;
       unsigned k = 0;
-      while (k < n && used + add + s_bytes[k] <= a.budget) add += s_bytes[k++];
-      if (add) atomicAdd(&a.dev->inflight, add);
+      bool locked = false;
+      const unsigned shift = s_nalloc ? hv(&a.heap.ctl->unit_shift) : 0u;
+      const unsigned nunits = s_nalloc ? hv(&a.heap.ctl->nunits) : 0u;
+      while (k < n) {
+        if (a.budget && used + add + s_bytes[k] > a.budget) break;
+        if (s_alloc[k]) {
+          if (!locked && !(locked = heap_lock(a.heap))) break;
+          b200shm_request *rq = &a.mreq[(from + k) % a.Q].r;
+          const unsigned long long units = heap_units(dest_bytes(*(const b200shm_request *)rq), shift);
+          const unsigned u = units <= nunits ? heap_alloc_locked(a.heap, (unsigned)(units ? units : 1), 1)
+                                             : kHeapNil;
+          if (u == kHeapNil) break; /* waits for room: frees or completions */
+          *(volatile unsigned long long *)&rq->dest_off = (unsigned long long)u << shift;
+        }
+        add += s_bytes[k++];
+      }
+      if (locked) heap_unlock(a.heap);
+      if (a.budget && add) atomicAdd(&a.dev->inflight, add);
       s_admit = k;
     }
     __syncthreads();
@@ -771,7 +810,10 @@ __global__ void __launch_bounds__(kServeThreads) k_serve(const SArgs a) {
         fence_sys();
         a.tiles_done[slot] = 0;
         SDone *dn = &a.done[slot];
-        *(volatile unsigned long long *)&dn->fetched = s_fetched;
+        /* AMOs: the old value; other kinds: the dest offset they wrote to
+         * (the one the loop allocated, for B200SHM_SERVE_ALLOC) */
+        *(volatile unsigned long long *)&dn->fetched =
+            q.r.kind == B200SHM_REQ_AMO ? s_fetched : q.r.dest_off;
         *(volatile unsigned long long *)&dn->t[0] = q.pad;
         *(volatile unsigned long long *)&dn->t[1] = s_tclaim;
         *(volatile unsigned long long *)&dn->t[2] = now_ns();
@@ -848,6 +890,8 @@ int plan_request(const b200shm_request &r0, SReq *q) {
   b200shm_request &r = q->r;
   int rc = B200SHM_OK;
   const State &S = st();
+  /* the loop allocates the dest at admission: no dest to check here */
+  const bool alloc = r.dest_off == B200SHM_SERVE_ALLOC;
   switch (r.kind) {
   case B200SHM_REQ_REDUCE: {
     if ((rc = check_team(r.pe_start, r.pe_stride, r.pe_size))) return rc;
@@ -866,9 +910,9 @@ int plan_request(const b200shm_request &r0, SReq *q) {
     if (r.n > S.slice / es) return fail(B200SHM_ERR_ARG, "serve: nelems too large");
     const uint64_t bytes = r.n * es;
     if ((rc = check_extent(r.src_off, bytes, "serve reduce source")) ||
-        (rc = check_extent(r.dest_off, bytes, "serve reduce dest")))
+        (!alloc && (rc = check_extent(r.dest_off, bytes, "serve reduce dest"))))
       return rc;
-    if (r.dest_off != r.src_off && overlaps(r.dest_off, bytes, r.src_off, bytes))
+    if (!alloc && r.dest_off != r.src_off && overlaps(r.dest_off, bytes, r.src_off, bytes))
       return fail(B200SHM_ERR_ARG, "serve: reduce dest and source overlap");
     uint64_t unit = reduce_tile_read() / ((uint64_t)r.pe_size * es);
     unit = (unit + kServeThreads - 1) / kServeThreads * kServeThreads;
@@ -884,9 +928,9 @@ int plan_request(const b200shm_request &r0, SReq *q) {
     if (r.n > S.slice / P) return fail(B200SHM_ERR_ARG, "serve: block too large");
     const uint64_t sb = r.kind == B200SHM_REQ_FCOLLECT ? r.n : P * r.n;
     if ((rc = check_extent(r.src_off, sb, "serve source")) ||
-        (rc = check_extent(r.dest_off, P * r.n, "serve dest")))
+        (rc = check_extent(alloc ? 0 : r.dest_off, P * r.n, "serve dest")))
       return rc;
-    if (overlaps(r.dest_off, P * r.n, r.src_off, sb))
+    if (!alloc && overlaps(r.dest_off, P * r.n, r.src_off, sb))
       return fail(B200SHM_ERR_ARG, "serve: dest and source overlap");
     q->nseg = P * P;
     break;
@@ -896,16 +940,17 @@ int plan_request(const b200shm_request &r0, SReq *q) {
     if (r.pe_start < 0 || r.pe_start >= S.npes || r.pe < 0 || r.pe >= S.npes)
       return fail(B200SHM_ERR_ARG, "serve: PE out of range");
     if ((rc = check_extent(r.src_off, r.n, "serve source")) ||
-        (rc = check_extent(r.dest_off, r.n, "serve dest")))
+        (rc = check_extent(alloc ? 0 : r.dest_off, r.n, "serve dest")))
       return rc;
     const int dpe = r.kind == B200SHM_REQ_PUT ? r.pe : r.pe_start;
     const int spe = r.kind == B200SHM_REQ_PUT ? r.pe_start : r.pe;
-    if (dpe == spe && overlaps(r.dest_off, r.n, r.src_off, r.n))
+    if (!alloc && dpe == spe && overlaps(r.dest_off, r.n, r.src_off, r.n))
       return fail(B200SHM_ERR_ARG, "serve: dest and source overlap");
     q->nseg = 1;
     break;
   }
   case B200SHM_REQ_AMO: {
+    if (alloc) return fail(B200SHM_ERR_ARG, "serve: an atomic needs an existing target");
     if (r.pe < 0 || r.pe >= S.npes) return fail(B200SHM_ERR_ARG, "serve: AMO PE out of range");
     if (r.op < 0 || r.op >= B200SHM_AMO_NOP) return fail(B200SHM_ERR_ARG, "serve: AMO op %d", r.op);
     const bool w4 = r.dtype == B200SHM_I32 || r.dtype == B200SHM_U32 || r.dtype == B200SHM_F32;
@@ -1017,6 +1062,7 @@ int b200shm_serve_start_budget(uint32_t queue_slots, int ctas, double idle_secon
   a.npes = st().npes;
   a.idle_ns = (unsigned long long)(idle * 1e9);
   a.budget = heap_budget;
+  a.heap = heap_dev();
   a.mirror_batch = kMirrorBatch;
   if (const char *mb = getenv("B200SHM_SERVE_MIRROR_BATCH"))
     if (atoi(mb) > 0) a.mirror_batch = (unsigned)std::min(atoi(mb), (int)kMirrorMax);
@@ -1228,6 +1274,66 @@ int b200shm_serve_replay(b200shm_server *s, const b200shm_request *reqs, uint64_
     }
   }
   return B200SHM_OK;
+}
+
+int b200shm_serve_replay_ordered(const b200shm_request *reqs, uint64_t n, void *stream,
+                                 double *seconds, uint64_t *fetched) {
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (n && !reqs) return fail(B200SHM_ERR_ARG, "serve_replay_ordered: null requests");
+  cudaStream_t s = pick_stream(stream);
+  unsigned long long *h_f = nullptr, *d_f = nullptr;
+  if (n) {
+    B200_CK(cudaHostAlloc((void **)&h_f, n * sizeof(unsigned long long), cudaHostAllocMapped));
+    cudaError_t e = cudaHostGetDevicePointer((void **)&d_f, h_f, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(h_f);
+      return cuda_fail(e, "serve_replay_ordered");
+    }
+    memset(h_f, 0, n * sizeof(unsigned long long));
+  }
+  B200_CK(cudaStreamSynchronize(s));
+  const double t0 = host_now();
+  int rc = B200SHM_OK;
+  for (uint64_t k = 0; k < n && rc == B200SHM_OK; k++) {
+    const b200shm_request &r = reqs[k];
+    switch (r.kind) {
+    case B200SHM_REQ_REDUCE:
+      rc = b200shm_reduce(r.op, r.dtype, r.algo, r.pe_start, r.pe_stride, r.pe_size, r.dest_off,
+                          r.src_off, r.n, s);
+      break;
+    case B200SHM_REQ_FCOLLECT:
+      rc = b200shm_fcollect(r.pe_start, r.pe_stride, r.pe_size, r.dest_off, r.src_off, r.n, s);
+      break;
+    case B200SHM_REQ_ALLTOALL:
+      rc = b200shm_alltoall(r.pe_start, r.pe_stride, r.pe_size, r.dest_off, r.src_off, r.n, s);
+      break;
+    case B200SHM_REQ_PUT:
+    case B200SHM_REQ_GET: {
+      const int dpe = r.kind == B200SHM_REQ_PUT ? r.pe : r.pe_start;
+      const int spe = r.kind == B200SHM_REQ_PUT ? r.pe_start : r.pe;
+      void *d = b200shm_ptr(dpe, r.dest_off);
+      const void *sp = b200shm_ptr(spe, r.src_off);
+      rc = (d && sp) ? b200shm_memcpy(d, sp, r.n, s)
+                     : fail(B200SHM_ERR_ARG, "serve_replay_ordered: bad put/get");
+      break;
+    }
+    case B200SHM_REQ_AMO:
+      rc = amo_one_launch(r.op, r.dtype, r.pe, r.dest_off, r.value, r.cond, d_f + k, s);
+      break;
+    default: rc = fail(B200SHM_ERR_ARG, "serve_replay_ordered: request kind %d", r.kind);
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  const double t1 = host_now();
+  if (rc == B200SHM_OK && e != cudaSuccess) rc = cuda_fail(e, "serve_replay_ordered");
+  if (rc == B200SHM_OK) rc = take_status("serve_replay_ordered");
+  if (rc == B200SHM_OK) {
+    if (seconds) *seconds = t1 - t0;
+    if (fetched)
+      for (uint64_t k = 0; k < n; k++) fetched[k] = h_f[k];
+  }
+  if (h_f) cudaFreeHost(h_f);
+  return rc;
 }
 
 }  // extern "C"

@@ -16,6 +16,7 @@
  * pSync to SHMEM_SYNC_VALUE.
  */
 #include <stdint.h>
+#include <string.h>
 
 #include <atomic>
 #include <vector>
@@ -273,3 +274,155 @@ int64_t b200shm_barrier_flags_nonzero(void) {
 }
 
 }  // extern "C"
+
+/* ---------------------------------------------------------------------------
+ * Point-to-point synchronisation: the comparisons behind shmem_<T>_test,
+ * test_all/any/some[_vector] and (polled) wait_until* (src/shmemc/ucx/
+ * test.c:10-170, waituntil.c:18-320).  One launch compares a whole vector of
+ * symmetric words with acquire loads, so words written by the engine's
+ * puts, atomics and serving loop are seen.
+ * ------------------------------------------------------------------------- */
+namespace b200 {
+namespace {
+
+template <class T>
+__device__ __forceinline__ T ld_acquire_word(const T *p) {
+  if constexpr (sizeof(T) == 8) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return (T)v;
+  } else if constexpr (sizeof(T) == 4) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return (T)v;
+  } else {
+    unsigned short v;
+    asm volatile("ld.acquire.gpu.global.u16 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
+    return (T)v;
+  }
+}
+
+/* out[i] = 1 when vars[i] cmp value (values[i] for the vector forms),
+ * 0 when not, 2 when status[i] excludes it; loaded[i] = the bits read */
+template <class T>
+__global__ void __launch_bounds__(256) k_test_words(const T *vars, uint64_t n, int cmp, T value,
+                                                    const T *values, const int *status,
+                                                    unsigned char *out,
+                                                    unsigned long long *loaded) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (status && status[i] != 0) {
+      out[i] = 2;
+      continue;
+    }
+    const T x = ld_acquire_word(vars + i);
+    const T v = values ? values[i] : value;
+    bool r;
+    switch (cmp) {
+    case 0: r = x == v; break; /* SHMEM_CMP_EQ */
+    case 1: r = x != v; break; /* NE */
+    case 2: r = x > v; break;  /* GT */
+    case 3: r = x <= v; break; /* LE */
+    case 4: r = x < v; break;  /* LT */
+    default: r = x >= v; break; /* GE */
+    }
+    out[i] = r ? 1 : 0;
+    if (loaded) {
+      unsigned long long bits = 0;
+      memcpy(&bits, &x, sizeof(T));
+      loaded[i] = bits;
+    }
+  }
+}
+
+/* per-thread mapped staging for the host arrays of b200shm_test_words */
+struct TestStage {
+  char *h = nullptr, *d = nullptr;
+  size_t cap = 0;
+  ~TestStage() {
+    if (h) cudaFreeHost(h);
+  }
+};
+
+}  // namespace
+}  // namespace b200
+
+extern "C" int b200shm_test_words(int cmp, int dtype, int pe, uint64_t off, uint64_t nelems,
+                                  const int *status, const void *cmp_value,
+                                  const void *cmp_values, uint8_t *out, uint64_t *loaded) {
+  using namespace b200;
+  if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
+  if (cmp < 0 || cmp > 5) return fail(B200SHM_ERR_ARG, "test: unknown comparison %d", cmp);
+  uint64_t w;
+  switch (dtype) {
+  case B200SHM_I16: case B200SHM_U16: w = 2; break;
+  case B200SHM_I32: case B200SHM_U32: w = 4; break;
+  case B200SHM_I64: case B200SHM_U64: w = 8; break;
+  default: return fail(B200SHM_ERR_UNSUPPORTED, "test: dtype %d is not a 2/4/8-byte integer", dtype);
+  }
+  if (nelems == 0) return B200SHM_OK;
+  if (!out || (!cmp_value && !cmp_values))
+    return fail(B200SHM_ERR_ARG, "test: missing result or comparison value");
+  if (pe < 0 || pe >= st().npes || off % w || nelems > st().slice / w ||
+      off > st().slice - nelems * w)
+    return fail(B200SHM_ERR_ARG, "test: %llu words at (PE %d, offset %llu) are not in the heap",
+                (unsigned long long)nelems, pe, (unsigned long long)off);
+  static thread_local TestStage stg;
+  /* layout: out bytes | status ints | values | loaded words, 16-byte aligned parts */
+  auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  const size_t o_st = up16(nelems), o_val = o_st + up16(status ? nelems * 4 : 0);
+  const size_t o_ld = o_val + up16(cmp_values ? nelems * w : 0);
+  const size_t need = o_ld + (loaded ? nelems * 8 : 0) + 16;
+  if (need > stg.cap) {
+    if (stg.h) cudaFreeHost(stg.h);
+    stg.h = stg.d = nullptr;
+    stg.cap = 0;
+    size_t cap = need < 4096 ? 4096 : need;
+    B200_CK(cudaHostAlloc((void **)&stg.h, cap, cudaHostAllocMapped));
+    cudaError_t e = cudaHostGetDevicePointer((void **)&stg.d, stg.h, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "test staging");
+    stg.cap = cap;
+  }
+  if (status) memcpy(stg.h + o_st, status, nelems * 4);
+  if (cmp_values) memcpy(stg.h + o_val, cmp_values, nelems * w);
+  const char *vars = st().base + (uint64_t)pe * st().slice + off;
+  const int *d_st = status ? (const int *)(stg.d + o_st) : nullptr;
+  unsigned char *d_out = (unsigned char *)stg.d;
+  unsigned long long *d_ld = loaded ? (unsigned long long *)(stg.d + o_ld) : nullptr;
+  cudaStream_t s = st().stream;
+  const unsigned grid = grid_for(nelems, 256, 4);
+  uint64_t v = 0;
+  if (cmp_value) memcpy(&v, cmp_value, w);
+  switch (dtype) {
+  case B200SHM_I16:
+    k_test_words<int16_t><<<grid, 256, 0, s>>>((const int16_t *)vars, nelems, cmp, (int16_t)v,
+        cmp_values ? (const int16_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  case B200SHM_U16:
+    k_test_words<uint16_t><<<grid, 256, 0, s>>>((const uint16_t *)vars, nelems, cmp, (uint16_t)v,
+        cmp_values ? (const uint16_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  case B200SHM_I32:
+    k_test_words<int32_t><<<grid, 256, 0, s>>>((const int32_t *)vars, nelems, cmp, (int32_t)v,
+        cmp_values ? (const int32_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  case B200SHM_U32:
+    k_test_words<uint32_t><<<grid, 256, 0, s>>>((const uint32_t *)vars, nelems, cmp, (uint32_t)v,
+        cmp_values ? (const uint32_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  case B200SHM_I64:
+    k_test_words<int64_t><<<grid, 256, 0, s>>>((const int64_t *)vars, nelems, cmp, (int64_t)v,
+        cmp_values ? (const int64_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  default:
+    k_test_words<uint64_t><<<grid, 256, 0, s>>>((const uint64_t *)vars, nelems, cmp, (uint64_t)v,
+        cmp_values ? (const uint64_t *)(stg.d + o_val) : nullptr, d_st, d_out, d_ld);
+    break;
+  }
+  count_launch();
+  const int rc = finish(nullptr, "b200shm_test_words");
+  if (rc) return rc;
+  memcpy(out, stg.h, nelems);
+  if (loaded) memcpy(loaded, stg.h + o_ld, nelems * 8);
+  return B200SHM_OK;
+}

@@ -448,7 +448,7 @@ void shmem_free(void *ptr) {
   arrive(&g_world, &r);
 }
 void *shmem_ptr(const void *dest, int pe) {
-  uint64_t off;
+  uint64_t off = 0;
   if (sym_off(dest, &off) || pe < 0 || pe >= g_npes) return NULL;
   return b200shm_ptr(pe, off);
 }
@@ -599,7 +599,7 @@ static int nbi_rma(nbi_list_t *l, int kind, void *dest, const void *source, size
 
 static void nbi_amo(nbi_list_t *l, int op, int dtype, const void *dest, int pe,
                     const void *value, const void *cond, void *fetch, int size) {
-  uint64_t off;
+  uint64_t off = 0;
   if (sym_off(dest, &off)) {
     t_status = B200SHM_ERR_ARG;
     return;
@@ -621,11 +621,11 @@ static void nbi_amo(nbi_list_t *l, int op, int dtype, const void *dest, int pe,
 }
 
 void shmem_putmem(void *dest, const void *source, size_t nelems, int pe) {
-  uint64_t off;
+  uint64_t off = 0;
   if (sym_off(dest, &off) == 0) t_status = engine_err(b200shm_memcpy(b200shm_ptr(pe, off), source, nelems, NULL));
 }
 void shmem_getmem(void *dest, const void *source, size_t nelems, int pe) {
-  uint64_t off;
+  uint64_t off = 0;
   if (sym_off(source, &off) == 0) t_status = engine_err(b200shm_memcpy(dest, b200shm_ptr(pe, off), nelems, NULL));
 }
 void shmem_ctx_putmem_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
@@ -1036,7 +1036,7 @@ DEF_SIZED(64)
 /* ---- atomics ------------------------------------------------------------------ */
 static void amo(int op, int dtype, const void *dest, int pe, const void *value, const void *cond,
                 void *fetched) {
-  uint64_t off;
+  uint64_t off = 0;
   if (sym_off(dest, &off)) {
     t_status = B200SHM_ERR_ARG;
     return;
@@ -1268,3 +1268,387 @@ SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_BIT)
 SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_NBI_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_NBI_BIT)
+
+/* ---- strided and signalled RMA (src/api/rma/putget.h:131-220, 420;
+ *      put_signal.h:28-98, put_signal.c:67-285) ------------------------------- */
+static void iput_bytes(void *dest, const void *source, ptrdiff_t tst, ptrdiff_t sst,
+                       size_t nelems, size_t esize, int pe) {
+  uint64_t off = 0;
+  if (sym_off(dest, &off)) {
+    t_status = B200SHM_ERR_ARG;
+    return;
+  }
+  void *remote = b200shm_ptr(pe, off);
+  if (!remote) {
+    t_status = set_err(B200SHM_ERR_ARG, "iput: PE %d is not in the job", pe);
+    return;
+  }
+  t_status = engine_err(b200shm_memcpy_strided(remote, tst, source, sst, esize, nelems, NULL));
+}
+static void iget_bytes(void *dest, const void *source, ptrdiff_t tst, ptrdiff_t sst,
+                       size_t nelems, size_t esize, int pe) {
+  uint64_t off = 0;
+  if (sym_off(source, &off)) {
+    t_status = B200SHM_ERR_ARG;
+    return;
+  }
+  const void *remote = b200shm_ptr(pe, off);
+  if (!remote) {
+    t_status = set_err(B200SHM_ERR_ARG, "iget: PE %d is not in the job", pe);
+    return;
+  }
+  t_status = engine_err(b200shm_memcpy_strided(dest, tst, remote, sst, esize, nelems, NULL));
+}
+
+/* The data is delivered (a blocking copy) before the signal word is set
+ * or added to, so a PE that sees the signal sees the data; the _nbi forms
+ * complete the same way before they return. */
+static void put_signal(void *dest, const void *source, size_t nbytes, uint64_t *sig_addr,
+                       uint64_t signal, int sig_op, int pe) {
+  if (sig_op != SHMEM_SIGNAL_SET && sig_op != SHMEM_SIGNAL_ADD) {
+    t_status = set_err(B200SHM_ERR_ARG, "put_signal: unknown signal operation %d", sig_op);
+    return;
+  }
+  shmem_putmem(dest, source, nbytes, pe);
+  if (t_status) return;
+  amo(sig_op == SHMEM_SIGNAL_ADD ? B200SHM_AMO_ADD : B200SHM_AMO_SET, B200SHM_U64, sig_addr, pe,
+      &signal, NULL, NULL);
+}
+
+#define DEF_RMA_STRIDED(_type, _tn)                                            \
+  void shmem_##_tn##_iput(_type *dest, const _type *source, ptrdiff_t tst,     \
+                          ptrdiff_t sst, size_t nelems, int pe) {              \
+    iput_bytes(dest, source, tst, sst, nelems, sizeof(_type), pe);             \
+  }                                                                            \
+  void shmem_##_tn##_iget(_type *dest, const _type *source, ptrdiff_t tst,     \
+                          ptrdiff_t sst, size_t nelems, int pe) {              \
+    iget_bytes(dest, source, tst, sst, nelems, sizeof(_type), pe);             \
+  }                                                                            \
+  void shmem_ctx_##_tn##_iput(shmem_ctx_t ctx, _type *dest,                    \
+                              const _type *source, ptrdiff_t tst,              \
+                              ptrdiff_t sst, size_t nelems, int pe) {          \
+    iput_bytes(dest, source, tst, sst, nelems, sizeof(_type), ctx_pe(ctx, pe)); \
+  }                                                                            \
+  void shmem_ctx_##_tn##_iget(shmem_ctx_t ctx, _type *dest,                    \
+                              const _type *source, ptrdiff_t tst,              \
+                              ptrdiff_t sst, size_t nelems, int pe) {          \
+    iget_bytes(dest, source, tst, sst, nelems, sizeof(_type), ctx_pe(ctx, pe)); \
+  }                                                                            \
+  void shmem_##_tn##_put_signal(_type *dest, const _type *source,              \
+                                size_t nelems, uint64_t *sig_addr,             \
+                                uint64_t signal, int sig_op, int pe) {         \
+    put_signal(dest, source, nelems * sizeof(_type), sig_addr, signal, sig_op, \
+               pe);                                                            \
+  }                                                                            \
+  void shmem_##_tn##_put_signal_nbi(_type *dest, const _type *source,          \
+                                    size_t nelems, uint64_t *sig_addr,         \
+                                    uint64_t signal, int sig_op, int pe) {     \
+    put_signal(dest, source, nelems * sizeof(_type), sig_addr, signal, sig_op, \
+               pe);                                                            \
+  }                                                                            \
+  void shmem_ctx_##_tn##_put_signal(shmem_ctx_t ctx, _type *dest,              \
+                                    const _type *source, size_t nelems,        \
+                                    uint64_t *sig_addr, uint64_t signal,       \
+                                    int sig_op, int pe) {                      \
+    put_signal(dest, source, nelems * sizeof(_type), sig_addr, signal, sig_op, \
+               ctx_pe(ctx, pe));                                               \
+  }                                                                            \
+  void shmem_ctx_##_tn##_put_signal_nbi(shmem_ctx_t ctx, _type *dest,          \
+                                        const _type *source, size_t nelems,    \
+                                        uint64_t *sig_addr, uint64_t signal,   \
+                                        int sig_op, int pe) {                  \
+    put_signal(dest, source, nelems * sizeof(_type), sig_addr, signal, sig_op, \
+               ctx_pe(ctx, pe));                                               \
+  }
+SHMEM_B200_RMA_TYPES(DEF_RMA_STRIDED)
+
+#define DEF_RMA_SIZED(_bits)                                                   \
+  void shmem_put##_bits(void *dest, const void *source, size_t nelems, int pe) { \
+    shmem_putmem(dest, source, nelems * (_bits / 8), pe);                      \
+  }                                                                            \
+  void shmem_get##_bits(void *dest, const void *source, size_t nelems, int pe) { \
+    shmem_getmem(dest, source, nelems * (_bits / 8), pe);                      \
+  }                                                                            \
+  void shmem_put##_bits##_nbi(void *dest, const void *source, size_t nelems,   \
+                              int pe) {                                        \
+    shmem_putmem_nbi(dest, source, nelems * (_bits / 8), pe);                  \
+  }                                                                            \
+  void shmem_get##_bits##_nbi(void *dest, const void *source, size_t nelems,   \
+                              int pe) {                                        \
+    shmem_getmem_nbi(dest, source, nelems * (_bits / 8), pe);                  \
+  }                                                                            \
+  void shmem_iput##_bits(void *dest, const void *source, ptrdiff_t tst,        \
+                         ptrdiff_t sst, size_t nelems, int pe) {               \
+    iput_bytes(dest, source, tst, sst, nelems, _bits / 8, pe);                 \
+  }                                                                            \
+  void shmem_iget##_bits(void *dest, const void *source, ptrdiff_t tst,        \
+                         ptrdiff_t sst, size_t nelems, int pe) {               \
+    iget_bytes(dest, source, tst, sst, nelems, _bits / 8, pe);                 \
+  }                                                                            \
+  void shmem_ctx_put##_bits(shmem_ctx_t ctx, void *dest, const void *source,   \
+                            size_t nelems, int pe) {                           \
+    shmem_ctx_putmem(ctx, dest, source, nelems * (_bits / 8), pe);             \
+  }                                                                            \
+  void shmem_ctx_get##_bits(shmem_ctx_t ctx, void *dest, const void *source,   \
+                            size_t nelems, int pe) {                           \
+    shmem_ctx_getmem(ctx, dest, source, nelems * (_bits / 8), pe);             \
+  }                                                                            \
+  void shmem_ctx_put##_bits##_nbi(shmem_ctx_t ctx, void *dest,                 \
+                                  const void *source, size_t nelems, int pe) { \
+    shmem_ctx_putmem_nbi(ctx, dest, source, nelems * (_bits / 8), pe);         \
+  }                                                                            \
+  void shmem_ctx_get##_bits##_nbi(shmem_ctx_t ctx, void *dest,                 \
+                                  const void *source, size_t nelems, int pe) { \
+    shmem_ctx_getmem_nbi(ctx, dest, source, nelems * (_bits / 8), pe);         \
+  }                                                                            \
+  void shmem_ctx_iput##_bits(shmem_ctx_t ctx, void *dest, const void *source,  \
+                             ptrdiff_t tst, ptrdiff_t sst, size_t nelems,      \
+                             int pe) {                                         \
+    iput_bytes(dest, source, tst, sst, nelems, _bits / 8, ctx_pe(ctx, pe));    \
+  }                                                                            \
+  void shmem_ctx_iget##_bits(shmem_ctx_t ctx, void *dest, const void *source,  \
+                             ptrdiff_t tst, ptrdiff_t sst, size_t nelems,      \
+                             int pe) {                                         \
+    iget_bytes(dest, source, tst, sst, nelems, _bits / 8, ctx_pe(ctx, pe));    \
+  }                                                                            \
+  void shmem_put##_bits##_signal(void *dest, const void *source,               \
+                                 size_t nelems, uint64_t *sig_addr,            \
+                                 uint64_t signal, int sig_op, int pe) {        \
+    put_signal(dest, source, nelems * (_bits / 8), sig_addr, signal, sig_op,   \
+               pe);                                                            \
+  }                                                                            \
+  void shmem_put##_bits##_signal_nbi(void *dest, const void *source,           \
+                                     size_t nelems, uint64_t *sig_addr,        \
+                                     uint64_t signal, int sig_op, int pe) {    \
+    put_signal(dest, source, nelems * (_bits / 8), sig_addr, signal, sig_op,   \
+               pe);                                                            \
+  }                                                                            \
+  void shmem_ctx_put##_bits##_signal(shmem_ctx_t ctx, void *dest,              \
+                                     const void *source, size_t nelems,        \
+                                     uint64_t *sig_addr, uint64_t signal,      \
+                                     int sig_op, int pe) {                     \
+    put_signal(dest, source, nelems * (_bits / 8), sig_addr, signal, sig_op,   \
+               ctx_pe(ctx, pe));                                               \
+  }                                                                            \
+  void shmem_ctx_put##_bits##_signal_nbi(shmem_ctx_t ctx, void *dest,          \
+                                         const void *source, size_t nelems,    \
+                                         uint64_t *sig_addr, uint64_t signal,  \
+                                         int sig_op, int pe) {                 \
+    put_signal(dest, source, nelems * (_bits / 8), sig_addr, signal, sig_op,   \
+               ctx_pe(ctx, pe));                                               \
+  }
+DEF_RMA_SIZED(8)
+DEF_RMA_SIZED(16)
+DEF_RMA_SIZED(32)
+DEF_RMA_SIZED(64)
+DEF_RMA_SIZED(128)
+
+void shmem_putmem_signal(void *dest, const void *source, size_t nelems, uint64_t *sig_addr,
+                         uint64_t signal, int sig_op, int pe) {
+  put_signal(dest, source, nelems, sig_addr, signal, sig_op, pe);
+}
+void shmem_putmem_signal_nbi(void *dest, const void *source, size_t nelems, uint64_t *sig_addr,
+                             uint64_t signal, int sig_op, int pe) {
+  put_signal(dest, source, nelems, sig_addr, signal, sig_op, pe);
+}
+void shmem_ctx_putmem_signal(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                             uint64_t *sig_addr, uint64_t signal, int sig_op, int pe) {
+  put_signal(dest, source, nelems, sig_addr, signal, sig_op, ctx_pe(ctx, pe));
+}
+void shmem_ctx_putmem_signal_nbi(shmem_ctx_t ctx, void *dest, const void *source, size_t nelems,
+                                 uint64_t *sig_addr, uint64_t signal, int sig_op, int pe) {
+  put_signal(dest, source, nelems, sig_addr, signal, sig_op, ctx_pe(ctx, pe));
+}
+
+/* ---- point-to-point synchronisation (the src/api/pt2pt_synch files over
+ *      src/shmemc/ucx/test.c and waituntil.c) -------------------------------
+ * Every pass is one device comparison of the whole vector
+ * (b200shm_test_words); the waits repeat passes, yielding between them.
+ * The reference's waits spin without bound; here SHMEM_B200_WAIT_TIMEOUT
+ * (seconds) may bound them: a wait that runs out returns with the status
+ * B200SHM_ERR_TIMEOUT (shmemx_b200_last_status), wait_until_any with
+ * SIZE_MAX. */
+typedef struct {
+  size_t ntrue, nlive, first;
+} pass_t;
+
+static double wait_limit(void) {
+  const char *e = getenv("SHMEM_B200_WAIT_TIMEOUT");
+  const double v = e ? atof(e) : 0.0;
+  return v > 0.0 ? v : -1.0;
+}
+
+/* one comparison pass; indices (may be NULL) receive the true elements */
+static int pass(int cmp, int dtype, const void *ivars, size_t n, const int *status,
+                const void *value, const void *values, size_t *indices, uint64_t *loaded,
+                pass_t *p) {
+  p->ntrue = p->nlive = 0;
+  p->first = SIZE_MAX;
+  if (n == 0) return 0;
+  uint64_t off = 0;
+  if (sym_off(ivars, &off)) return t_status = B200SHM_ERR_ARG;
+  uint8_t small[256];
+  uint8_t *out = n <= sizeof(small) ? small : (uint8_t *)malloc(n);
+  if (!out) return t_status = set_err(B200SHM_ERR_NOMEM, "test: out of host memory");
+  const int rc = engine_err(b200shm_test_words(cmp, dtype, t_pe, off, n, status, value, values,
+                                               out, loaded));
+  if (rc == 0) {
+    for (size_t i = 0; i < n; i++) {
+      if (out[i] == 2) continue;
+      p->nlive++;
+      if (out[i] == 1) {
+        if (p->first == SIZE_MAX) p->first = i;
+        if (indices) indices[p->ntrue] = i;
+        p->ntrue++;
+      }
+    }
+  }
+  if (out != small) free(out);
+  return t_status = rc;
+}
+
+enum { W_ONE, W_ALL, W_ANY, W_SOME };
+/* repeat passes until the wait's condition holds (or the bound runs out) */
+static int wait_pass(int kind, int cmp, int dtype, const void *ivars, size_t n,
+                     const int *status, const void *value, const void *values, size_t *indices,
+                     uint64_t *loaded, pass_t *p) {
+  const double limit = wait_limit(), t0 = shmemx_wtime();
+  for (unsigned it = 0;; it++) {
+    if (pass(cmp, dtype, ivars, n, status, value, values, indices, loaded, p)) return t_status;
+    if (kind == W_ALL ? p->ntrue == p->nlive : (p->ntrue > 0 || p->nlive == 0)) return 0;
+    if (limit > 0 && shmemx_wtime() - t0 > limit)
+      return t_status = set_err(B200SHM_ERR_TIMEOUT, "wait_until: not satisfied after %.3f s",
+                                limit);
+    if (it > 16) sched_yield();
+  }
+}
+
+#define DEF_SYNC_ONE(_type, _tn)                                               \
+  int shmem_##_tn##_test(_type *ivar, int cmp, _type cmp_value) {              \
+    pass_t p;                                                                  \
+    pass(cmp, B200_DTYPE_OF(_type), ivar, 1, NULL, &cmp_value, NULL, NULL,     \
+         NULL, &p);                                                            \
+    return p.ntrue ? 1 : 0;                                                    \
+  }                                                                            \
+  void shmem_##_tn##_wait_until(_type *ivar, int cmp, _type cmp_value) {       \
+    pass_t p;                                                                  \
+    wait_pass(W_ONE, cmp, B200_DTYPE_OF(_type), ivar, 1, NULL, &cmp_value,     \
+              NULL, NULL, NULL, &p);                                           \
+  }                                                                            \
+  void shmem_##_tn##_wait(_type *ivar, _type cmp_value) {                      \
+    shmem_##_tn##_wait_until(ivar, SHMEM_CMP_NE, cmp_value);                   \
+  }
+#define DEF_SYNC_VEC(_type, _tn)                                               \
+  int shmem_##_tn##_test_all(_type *ivars, size_t nelems, const int *status,   \
+                             int cmp, _type cmp_value) {                       \
+    pass_t p;                                                                  \
+    if (pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, &cmp_value,     \
+             NULL, NULL, NULL, &p))                                            \
+      return 0;                                                                \
+    return p.ntrue == p.nlive ? 1 : 0;                                         \
+  }                                                                            \
+  size_t shmem_##_tn##_test_any(_type *ivars, size_t nelems,                   \
+                                const int *status, int cmp, _type cmp_value) { \
+    pass_t p;                                                                  \
+    pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, &cmp_value, NULL,   \
+         NULL, NULL, &p);                                                      \
+    return p.first;                                                            \
+  }                                                                            \
+  size_t shmem_##_tn##_test_some(_type *ivars, size_t nelems, size_t *indices, \
+                                 const int *status, int cmp,                   \
+                                 _type cmp_value) {                            \
+    pass_t p;                                                                  \
+    pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, &cmp_value, NULL,   \
+         indices, NULL, &p);                                                   \
+    return p.ntrue;                                                            \
+  }                                                                            \
+  int shmem_##_tn##_test_all_vector(_type *ivars, size_t nelems,               \
+                                    const int *status, int cmp,                \
+                                    _type *cmp_values) {                       \
+    pass_t p;                                                                  \
+    if (pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, NULL,           \
+             cmp_values, NULL, NULL, &p))                                      \
+      return 0;                                                                \
+    return p.ntrue == p.nlive ? 1 : 0;                                         \
+  }                                                                            \
+  size_t shmem_##_tn##_test_any_vector(_type *ivars, size_t nelems,            \
+                                       const int *status, int cmp,             \
+                                       _type *cmp_values) {                    \
+    pass_t p;                                                                  \
+    pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, NULL, cmp_values,   \
+         NULL, NULL, &p);                                                      \
+    return p.first;                                                            \
+  }                                                                            \
+  size_t shmem_##_tn##_test_some_vector(_type *ivars, size_t nelems,           \
+                                        size_t *indices, const int *status,    \
+                                        int cmp, _type *cmp_values) {          \
+    pass_t p;                                                                  \
+    pass(cmp, B200_DTYPE_OF(_type), ivars, nelems, status, NULL, cmp_values,   \
+         indices, NULL, &p);                                                   \
+    return p.ntrue;                                                            \
+  }                                                                            \
+  void shmem_##_tn##_wait_until_all(_type *ivars, size_t nelems,               \
+                                    const int *status, int cmp,                \
+                                    _type cmp_value) {                         \
+    pass_t p;                                                                  \
+    wait_pass(W_ALL, cmp, B200_DTYPE_OF(_type), ivars, nelems, status,         \
+              &cmp_value, NULL, NULL, NULL, &p);                               \
+  }                                                                            \
+  size_t shmem_##_tn##_wait_until_any(_type *ivars, size_t nelems,             \
+                                      const int *status, int cmp,              \
+                                      _type cmp_value) {                       \
+    pass_t p;                                                                  \
+    if (wait_pass(W_ANY, cmp, B200_DTYPE_OF(_type), ivars, nelems, status,     \
+                  &cmp_value, NULL, NULL, NULL, &p))                           \
+      return SIZE_MAX;                                                         \
+    return p.first;                                                            \
+  }                                                                            \
+  size_t shmem_##_tn##_wait_until_some(_type *ivars, size_t nelems,            \
+                                       size_t *indices, const int *status,     \
+                                       int cmp, _type cmp_value) {             \
+    pass_t p;                                                                  \
+    if (wait_pass(W_SOME, cmp, B200_DTYPE_OF(_type), ivars, nelems, status,    \
+                  &cmp_value, NULL, indices, NULL, &p))                        \
+      return 0;                                                                \
+    return p.ntrue;                                                            \
+  }                                                                            \
+  void shmem_##_tn##_wait_until_all_vector(_type *ivars, size_t nelems,        \
+                                           const int *status, int cmp,         \
+                                           _type *cmp_values) {                \
+    pass_t p;                                                                  \
+    wait_pass(W_ALL, cmp, B200_DTYPE_OF(_type), ivars, nelems, status, NULL,   \
+              cmp_values, NULL, NULL, &p);                                     \
+  }                                                                            \
+  size_t shmem_##_tn##_wait_until_any_vector(_type *ivars, size_t nelems,      \
+                                             const int *status, int cmp,       \
+                                             _type *cmp_values) {              \
+    pass_t p;                                                                  \
+    if (wait_pass(W_ANY, cmp, B200_DTYPE_OF(_type), ivars, nelems, status,     \
+                  NULL, cmp_values, NULL, NULL, &p))                           \
+      return SIZE_MAX;                                                         \
+    return p.first;                                                            \
+  }                                                                            \
+  size_t shmem_##_tn##_wait_until_some_vector(_type *ivars, size_t nelems,     \
+                                              size_t *indices,                 \
+                                              const int *status, int cmp,      \
+                                              _type *cmp_values) {             \
+    pass_t p;                                                                  \
+    if (wait_pass(W_SOME, cmp, B200_DTYPE_OF(_type), ivars, nelems, status,    \
+                  NULL, cmp_values, indices, NULL, &p))                        \
+      return 0;                                                                \
+    return p.ntrue;                                                            \
+  }
+SHMEM_B200_SYNC_TYPES(DEF_SYNC_ONE)
+SHMEM_B200_AMO_STANDARD_TYPES(DEF_SYNC_VEC)
+
+uint64_t shmem_signal_fetch(const uint64_t *sig_addr) {
+  uint64_t v = 0;
+  amo(B200SHM_AMO_FETCH, B200SHM_U64, sig_addr, t_pe, NULL, NULL, &v);
+  return v;
+}
+uint64_t shmem_signal_wait_until(uint64_t *sig_addr, int cmp, uint64_t cmp_value) {
+  pass_t p;
+  uint64_t seen = 0;
+  wait_pass(W_ONE, cmp, B200SHM_U64, sig_addr, 1, NULL, &cmp_value, NULL, NULL, &seen, &p);
+  return seen;
+}

@@ -56,3 +56,23 @@ def test_shmem_surface_exports_every_declared_function():
     lib = ctypes.CDLL(host_lib)
     missing = sorted(n for n in names if not hasattr(lib, n))
     assert not missing, missing[:20]
+
+
+def test_every_openshmem_declaration_is_exported():
+    """include/shmem.h and shmemx.h generate most of their declarations from
+    type tables; every function they declare (after the preprocessor) is
+    exported by libshmem_b200.so."""
+    import subprocess
+    lib = ctypes.CDLL(os.path.join(ROOT, "osss-ucx_b200", "lib", "libshmem_b200.so"))
+    missing = []
+    for h in ("shmem.h", "shmemx.h"):
+        text = subprocess.run(["gcc", "-E", "-P", "-x", "c", os.path.join(ROOT, "include", h)],
+                              capture_output=True, text=True, check=True).stdout
+        names = sorted(set(re.findall(r"\b((?:shmem|shmemx|pshmem)_[A-Za-z0-9_]+)\s*\(", text)))
+        assert len(names) > (1000 if h == "shmem.h" else 4)
+        for name in names:
+            try:
+                getattr(lib, name)
+            except AttributeError:
+                missing.append((h, name))
+    assert not missing, missing[:20]

@@ -224,3 +224,23 @@ def test_spmd_contexts_quiet_independently(tmp_path):
     assert o["counter2"] == NN and sorted(o["fc"].tolist()) == list(range(NN))
     assert (o["invalid_status"] < 0).all()
     assert (o["g"] == np.arange(NN)).all()
+
+
+@pytest.mark.gpu
+def test_spmd_point_to_point_sync_and_signalled_puts(tmp_path):
+    """tests/c/spmd_sync.c checks itself: strided iput/iget (typed and
+    sized), put_signal with signal_wait_until / signal_fetch, the
+    test/wait_until families with status masks and vector compare values,
+    unsigned comparison, and that a collective whose members disagree fails
+    on every member with the same message."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_sync")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_sync.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    r = subprocess.run([exe], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M",
+                                       SHMEM_B200_WAIT_TIMEOUT="60"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
