@@ -1,0 +1,135 @@
+"""A team spanning GPUs (osss-ucx_b200/spanning.py), its cross-rank steps on
+CPU gloo ranks (world sizes 2, 3 and 4).  Each rank's local step -- on a GPU
+the engine's reduction over its members -- is stood in for here by the
+oracle's restatement over the same members, in the same order; the
+butterfly over ranks, the rank-order fold of a world that is not a power of
+two, the exactness rule and the write-back run as they do on GPUs.  The
+result is compared with the oracle over the whole team: bit for bit where
+`exact` says so, else within P * eps * sum|x|."""
+import os
+import socket
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# (op, dtype, algo, P)
+CASES = {
+    2: [("sum", "float32", "rec_dbl", 16), ("prod", "float64", "rabenseifner", 8),
+        ("sum", "float64", "rabenseifner2", 32), ("xor", "int64", "rec_dbl", 6),
+        ("min", "float32", "rec_dbl", 8), ("sum", "float32", "linear", 8),
+        ("sum", "float64", "rec_dbl", 12)],
+    3: [("sum", "int32", "rec_dbl", 6), ("or", "uint64", "linear", 9),
+        ("sum", "float64", "rec_dbl", 6)],
+    4: [("sum", "float32", "rec_dbl", 16), ("sum", "float64", "rabenseifner", 64),
+        ("prod", "int64", "rec_dbl", 12), ("max", "float64", "linear", 8),
+        ("sum", "float32", "rec_dbl", 4)],
+}
+N = 1000
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def inputs(op, dtype, P, seed):
+    import gen
+    dt = np.dtype(dtype)
+    if dt.kind in "iu":
+        lo, hi = (-3, 3) if op == "prod" else (None, None)
+        if dt.kind == "u" and lo is not None:
+            lo = 0
+        return gen.uniform_int(dt, P, N, seed, lo, hi)
+    if op == "prod":
+        return gen.uniform(dt, P, N, seed, 0.99, 1.01)
+    return gen.normal(dt, P, N, seed)
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    for p in (os.path.join(ROOT, "osss-ucx_b200"), os.path.join(ROOT, "oracle"),
+              os.path.join(ROOT, "tests")):
+        sys.path.insert(0, p)
+    import oracle
+    import spanning
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    rs = oracle.Restatement()
+
+    class OracleLocal(spanning.SpanningTeam):
+        """The local step by the oracle (CPU), the write-back into `out`."""
+
+        def local_partial(self, op, dtype, algo, dest, src, nelems):
+            return torch.from_numpy(np.ascontiguousarray(rs.reduce(algo, op, self.mine)[0]))
+
+        def write_back(self, result, dest, nelems, dtype):
+            self.out = result.numpy().copy()
+
+    res = []
+    for k, (op, dtype, algo, P) in enumerate(CASES[world]):
+        x = inputs(op, dtype, P, 100 * world + k)
+        per = P // world
+        team = OracleLocal(None, per)
+        team.mine = x[rank * per:(rank + 1) * per]
+        exact = team.reduce(op, dtype, algo, 0, 0, N)
+        want = rs.reduce(algo, op, x)[0]
+        if exact:
+            ok = team.out.tobytes() == want.tobytes()
+        else:
+            w64 = x.astype(np.float64)
+            exact_sum = w64.sum(0) if op == "sum" else w64.prod(0) if op == "prod" else want
+            bound = P * np.finfo(np.dtype(dtype)).eps * np.abs(w64).sum(0)
+            ok = bool((np.abs(team.out.astype(np.float64) - exact_sum) <= bound).all())
+        res.append((k, bool(exact), bool(ok)))
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, res))
+
+
+def run_world(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    ps = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    out = dict(q.get(timeout=300) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return out
+
+
+def expected_exact(op, dtype, algo, P, world):
+    if not dtype.startswith("float") or op in ("min", "max"):
+        return True
+    pow2 = lambda n: n & (n - 1) == 0
+    return algo in ("rec_dbl", "rabenseifner", "rabenseifner2") and pow2(P) and pow2(world)
+
+
+def check(world):
+    out = run_world(world)
+    for rank, res in out.items():
+        for k, exact, ok in res:
+            op, dtype, algo, P = CASES[world][k]
+            assert exact == expected_exact(op, dtype, algo, P, world), (world, CASES[world][k])
+            assert ok, (world, rank, CASES[world][k])
+
+
+def test_two_ranks():
+    check(2)
+
+
+def test_three_ranks_fold_in_rank_order():
+    check(3)
+
+
+def test_four_ranks():
+    check(4)
