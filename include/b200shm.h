@@ -256,21 +256,26 @@ typedef struct b200shm_reduce_desc {
 
 typedef struct b200shm_batch b200shm_batch;
 
-#define B200SHM_BATCH_NO_TUNE 0x1 /* the heuristic plan (the default)      */
+#define B200SHM_BATCH_NO_TUNE 0x1 /* the heuristic plan (or cached choices) only */
 #define B200SHM_BATCH_GRAPH 0x2   /* capture the run into a CUDA graph     */
-#define B200SHM_BATCH_TUNE 0x4    /* time candidate plans per shape class  */
+#define B200SHM_BATCH_TUNE 0x4    /* tune (the default unless NO_TUNE)     */
 
 /* Plan a batch of n independent reductions: validate every descriptor,
- * choose lanes per column, columns per lane and tile size per shape (by the
- * measured heuristic, or with B200SHM_BATCH_TUNE by timing candidates on
- * the device the first time a shape class is seen, cached for the process;
- * the heuristic measured faster on mixed batches), and upload the plan.  The reductions run
+ * choose lanes per column, columns per lane and tile size per shape (the
+ * autotuner's cached choice for the shape's class, else a measured
+ * heuristic), then -- unless B200SHM_BATCH_NO_TUNE, or a descriptor runs
+ * in place -- tune: for the shape classes that carry the most bytes and
+ * have no cached choice, try the other (lanes, tile) plans and time the
+ * whole batch as it runs, keeping what makes it faster; the choices are
+ * cached for the process.  Tuning runs the batch, so the dests are written
+ * at create time (with the values a run writes).  The reductions run
  * concurrently, so a descriptor whose dest touches another descriptor's
  * source or dest (in any member) is rejected with B200SHM_ERR_ARG; sharing
  * a source, and a descriptor in place, are fine.  Replaces n separate
  * shcoll_<T>_<op>_reduce_<algo> calls (src/shcoll/src/reduce.c:1078-1102),
  * which the reference can only issue one after the other.  Every result is
- * bit-identical to b200shm_reduce on the same descriptor. */
+ * bit-identical to b200shm_reduce on the same descriptor, whatever the
+ * plan. */
 int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
                          b200shm_batch **out);
 /* Run the whole batch: one persistent launch per (type, op, combine order)

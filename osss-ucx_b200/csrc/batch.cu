@@ -18,8 +18,9 @@
  * SUM/PROD, deferral plus exact replay for order-dependent float MIN/MAX
  * elements).  Per descriptor the plan picks the lanes per 16-byte column
  * G, the columns per lane U (small teams serve 2 or 4 columns at once so a
- * lane keeps ~8 loads in flight) and the tile size; an optional autotuner
- * times candidate (G, tile) plans per shape class instead.
+ * lane keeps ~8 loads in flight) and the tile size, by a measured
+ * heuristic, and then (by default) an autotuner that times candidate
+ * (G, tile) plans per shape class inside the whole batch as it runs.
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -59,7 +60,7 @@ struct BDesc {
   int P, p2s, logp2s, algo;
   int kid, vec, G, TP; /* TP: packs (vec) or elements (!vec) per tile */
   int U;               /* columns each lane serves at once (small teams) */
-  int pad;
+  int id;              /* index of the caller's descriptor */
 };
 
 struct BPlan {
@@ -496,7 +497,7 @@ struct Shape {
   }
 };
 std::mutex g_tune_mu;
-std::map<Shape, std::pair<int, int>> g_tune; /* shape -> (G, TP) */
+std::map<Shape, std::pair<int, int>> g_tune; /* shape -> (G, TP), chosen by the autotuner */
 
 int log2_floor(uint64_t x) {
   int l = 0;
@@ -517,6 +518,13 @@ inline int esize_of(const BDesc &d) {
 inline bool is_mm_float(const BDesc &d) {
   return ds_of(d) >= DS_F32 && (op_of(d) == B200SHM_MIN || op_of(d) == B200SHM_MAX);
 }
+/* the shape class a plan is chosen (and cached) for */
+inline Shape shape_of(const BDesc &d) {
+  return Shape{order_of(d) * 2 + (is_mm_float(d) ? 1 : 0), esize_of(d),
+               log2_floor((uint64_t)d.P), log2_floor(d.N) / 2, d.vec};
+}
+/* shape classes the autotuner tries, the heaviest (by bytes) first */
+constexpr size_t kTuneClasses = 8;
 
 /* Columns per lane for small teams: enough that a lane keeps about 8
  * loads in flight (chains: members per lane <= 2 -> 4 columns, <= 4 -> 2;
@@ -754,45 +762,13 @@ int upload(Batch &b) {
   return B200SHM_OK;
 }
 
-/* Time one descriptor through the batch kernel under plan (G, TP). */
-float time_plan(const BDesc &d0, int G, int TP, cudaStream_t s) {
-  Batch t;
-  BDesc d = d0;
-  d.G = G;
-  d.TP = TP;
-  set_columns(d);
-  t.hd.push_back(d);
-  t.any_mm = is_mm_float(d);
-  float best = 1e30f;
-  if (upload(t) == B200SHM_OK) {
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    enqueue(t, s);
-    for (int r = 0; r < 3; r++) {
-      cudaEventRecord(e0, s);
-      enqueue(t, s);
-      cudaEventRecord(e1, s);
-      cudaEventSynchronize(e1);
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) best = ms;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-  }
-  release(t);
-  return best;
-}
-
-/* Choose (G, TP) for d: cached per shape, timed on first sight. */
-void choose_plan(BDesc &d, bool tune, cudaStream_t s) {
+/* The plan of d: the autotuner's choice for its shape class when one is
+ * cached, else the measured heuristic. */
+void choose_plan(BDesc &d) {
   const int order = order_of(d);
-  Shape key{order * 2 + (is_mm_float(d) ? 1 : 0), esize_of(d), log2_floor((uint64_t)d.P),
-            log2_floor(d.N) / 2, d.vec};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune.find(key);
+    auto it = g_tune.find(shape_of(d));
     if (it != g_tune.end() && lanes_ok(d, it->second.first)) {
       d.G = it->second.first;
       d.TP = it->second.second;
@@ -811,23 +787,102 @@ void choose_plan(BDesc &d, bool tune, cudaStream_t s) {
   while (!lanes_ok(d, G) && G < 8) G <<= 1;
   d.G = G;
   d.TP = 1024;
-  if (tune) {
-    float best = 1e30f;
-    const int tps[] = {128, 512, 2048, 8192};
+}
+
+/* One timing of the whole batch as planned in `base` (plan applied, then
+ * uploaded as a run uploads it): the best of three runs on stream s, ms. */
+float time_batch(Batch &b, const std::vector<BDesc> &base, cudaStream_t s) {
+  release(b);
+  b.hd = base;
+  for (BDesc &d : b.hd) set_columns(d);
+  if (upload(b) != B200SHM_OK || make_side(b) != B200SHM_OK) return 1e30f;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return 1e30f;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return 1e30f;
+  }
+  float best = 1e30f;
+  if (enqueue(b, s) == B200SHM_OK) {
+    for (int r = 0; r < 3; r++) {
+      cudaEventRecord(e0, s);
+      enqueue(b, s);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best) best = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+/* The autotuner, inside the batch as it runs.  Start from the current plan
+ * (cached choices, else the heuristic); then, for the shape classes that
+ * carry the most bytes and have no cached choice yet, one class at a time,
+ * give every descriptor of the class each other (lanes per column, tile)
+ * and time the WHOLE batch -- its groups overlapping on the side streams,
+ * as a run does -- keeping a change only when the batch got more than 1 %
+ * faster.  The choices go to the per-process cache, which later batches
+ * start from.  (Timing a shape class alone, where launch overhead
+ * dominates, chose plans that lost inside the mixed batch.)  Tuning runs
+ * the batch, so its dests are written, with the values a run writes; a
+ * batch with an in-place descriptor is not tuned.  Results do not depend
+ * on the plan: every plan keeps the algorithm's combine order. */
+void tune_batch(Batch &b, cudaStream_t s) {
+  std::vector<BDesc> base = b.hd;
+  std::map<Shape, std::pair<double, std::vector<size_t>>> cls;
+  for (size_t i = 0; i < base.size(); i++) {
+    const BDesc &d = base[i];
+    auto &c = cls[shape_of(d)];
+    c.first += 2.0 * d.P * (double)d.N * esize_of(d);
+    c.second.push_back(i);
+  }
+  std::vector<std::pair<double, Shape>> order;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto &kv : cls)
+      if (!g_tune.count(kv.first)) order.push_back({kv.second.first, kv.first});
+  }
+  std::sort(order.begin(), order.end(),
+            [](const std::pair<double, Shape> &x, const std::pair<double, Shape> &y) {
+              return x.first > y.first;
+            });
+  if (order.size() > kTuneClasses) order.resize(kTuneClasses);
+  float best = time_batch(b, base, s);
+  for (auto &oc : order) {
+    const std::vector<size_t> &idx = cls[oc.second].second;
+    int bestG = base[idx[0]].G, bestTP = base[idx[0]].TP;
     for (int g = 1; g <= 8; g <<= 1) {
-      if (!lanes_ok(d, g)) continue;
-      for (int tp : tps) {
-        const float ms = time_plan(d, g, tp, s);
-        if (ms < best) {
+      for (int tp : {256, 1024, 4096}) {
+        if (g == bestG && tp == bestTP) continue;
+        std::vector<BDesc> cand = base;
+        bool ok = true;
+        for (size_t i : idx) {
+          if (!lanes_ok(cand[i], g)) {
+            ok = false;
+            break;
+          }
+          cand[i].G = g;
+          cand[i].TP = tp;
+        }
+        if (!ok) continue;
+        const float ms = time_batch(b, cand, s);
+        if (ms < best * 0.99f) {
           best = ms;
-          d.G = g;
-          d.TP = tp;
+          base = cand;
+          bestG = g;
+          bestTP = tp;
         }
       }
     }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[oc.second] = {bestG, bestTP};
   }
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune[key] = {d.G, d.TP};
+  release(b);
+  b.hd = base;
+  for (BDesc &d : b.hd) set_columns(d);
 }
 
 /* The reductions of a batch run concurrently, so no descriptor's dest may
@@ -923,7 +978,7 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
     delete bh;
     return rc;
   };
-  const bool tune = (flags & B200SHM_BATCH_TUNE) && !(flags & B200SHM_BATCH_NO_TUNE);
+  bool tune = !(flags & B200SHM_BATCH_NO_TUNE);
   for (uint64_t i = 0; i < n; i++) {
     b200shm_reduce_desc &x = descs[i];
     if (x.algo == B200SHM_ALGO_AUTO) x.algo = B200SHM_REC_DBL;
@@ -982,12 +1037,13 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
     d.G = 1;
     d.TP = 1024;
     d.U = 1;
-    d.pad = 0;
+    d.id = (int)i;
     if (!lanes_ok(d, 1) && !lanes_ok(d, 2) && !lanes_ok(d, 4) && !lanes_ok(d, 8)) {
       b.fallback.push_back(x); /* trees deeper than one lane's stack */
       continue;
     }
-    choose_plan(d, tune, st().stream);
+    if (x.dest_off == x.src_off) tune = false; /* tuning runs the batch: not in place */
+    choose_plan(d);
     set_columns(d);
     x.lanes = d.G;
     x.tile = d.TP;
@@ -995,6 +1051,13 @@ int b200shm_batch_create(b200shm_reduce_desc *descs, uint64_t n, int flags,
     b.hd.push_back(d);
   }
   int rc = check_independent(descs, n);
+  if (!rc && tune && !b.hd.empty()) {
+    tune_batch(b, st().stream);
+    for (const BDesc &d : b.hd) { /* report the tuned plan */
+      descs[d.id].lanes = d.G;
+      descs[d.id].tile = d.TP;
+    }
+  }
   if (!rc) rc = upload(b);
   if (!rc) rc = make_side(b);
   if (!rc && cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming) != cudaSuccess)
@@ -1050,7 +1113,8 @@ int b200shm_batch_destroy(b200shm_batch *bh) {
 
 int b200shm_reduce_batch(b200shm_reduce_desc *descs, uint64_t n, void *stream) {
   b200shm_batch *b = nullptr;
-  int rc = b200shm_batch_create(descs, n, 0, &b);
+  /* one run: tuning would cost more than it could save */
+  int rc = b200shm_batch_create(descs, n, B200SHM_BATCH_NO_TUNE, &b);
   if (rc) return rc;
   rc = b200shm_batch_run(b, stream);
   if (stream) cudaStreamSynchronize((cudaStream_t)stream);

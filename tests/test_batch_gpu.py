@@ -83,6 +83,8 @@ def test_batch_matches_per_call_and_oracle(B, heap, rs, flags):
     descs = B.make_descs(items)
     b = B.Batch(descs, flags)
     for rep in range(2):
+        for it, x in zip(items, inputs):  # tuning ran the batch at create: clear again
+            B.memset(it["dest"], 0x5A, x[0].nbytes, team=it["team"])
         b.run()
         got = results(B, items, inputs)
         for k, (g, w) in enumerate(zip(got, want)):
@@ -173,3 +175,25 @@ def test_fill_uniform_is_seeded_and_in_range(B, heap):
     B.fill_uniform(off, "float32", 4096, 8, 0.999, 1.001, team=(0, 1, 4))
     f = B.get_rows(off, 4096 * 4, np.float32, team=(0, 1, 4))
     assert f.min() >= np.float32(0.999) and f.max() < np.float32(1.001)
+
+
+def test_tuned_plan_is_reported_and_exact(B, heap, rs):
+    """The autotuner (the default) times plans inside the whole batch; the
+    plan it reports per descriptor may differ from the heuristic's, and the
+    results are the same bits either way."""
+    rng = np.random.default_rng(99)
+    items, inputs = make_batch(B, heap, rng, 120, B.n_pes())
+    want = per_call(B, items, inputs)
+    heur = B.make_descs(items)
+    B.Batch(heur, B.BATCH_NO_TUNE).close()
+    tuned = B.make_descs(items)
+    b = B.Batch(tuned)
+    for it, x in zip(items, inputs):
+        B.memset(it["dest"], 0x5A, x[0].nbytes, team=it["team"])
+    b.run()
+    b.close()
+    got = results(B, items, inputs)
+    for k, (g, w) in enumerate(zip(got, want)):
+        assert g.tobytes() == w.tobytes(), (k, items[k])
+    assert all((d.lanes == 0) == (h.lanes == 0) for d, h in zip(tuned, heur))
+    assert all(d.tile in (0, 256, 1024, 4096) for d in tuned)
