@@ -15,6 +15,7 @@
  * multiple of 16, else in bytes (or elements for the strided form).
  */
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <vector>
 
@@ -56,6 +57,102 @@ __global__ void __launch_bounds__(256) k_fcollect(const char *src0, char *dst0, 
       for (int j = 0; j < P; j++) dst[(uint64_t)j * step + v] = c;
     }
   }
+}
+
+/* fcollect staged through shared memory with the bulk-copy engine: a CTA
+ * brings a tile of source k into shared memory with one cp.async.bulk load
+ * (completion counted on an mbarrier), then issues one cp.async.bulk store
+ * of the tile to each member's dest, so the P writes of every byte are
+ * issued by the copy engine rather than by P store instructions per thread.
+ * Two buffers: the load of the next tile overlaps the stores of this one.
+ * Needs 16-byte aligned offsets, step and size (the vector path's rule).
+ * Every wait is bounded; one that runs out sets the TIMEOUT status bit and
+ * the CTA stops issuing. */
+constexpr unsigned kFcBulkTile = 8192; /* bytes per tile */
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned phase) {
+  for (unsigned i = 0; i < (1u << 24); i++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(m)), "r"(phase)
+        : "memory");
+    if (ok) return true;
+    __nanosleep(32);
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void *dst_smem, const char *src, unsigned bytes,
+                                          uint64_t *m) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst_smem)),
+      "l"(src), "r"(bytes), "r"(smem_addr(m))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(256) k_fcollect_bulk(const char *src0, char *dst0,
+                                                       uint64_t step, int P, uint64_t nbytes,
+                                                       int *status) {
+  __shared__ __align__(128) char buf[2][kFcBulkTile];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ int s_ok;
+  const int k = blockIdx.y;
+  const char *src = src0 + (uint64_t)k * step;
+  const uint64_t ntiles = (nbytes + kFcBulkTile - 1) / kFcBulkTile;
+  uint64_t t = blockIdx.x;
+  if (t >= ntiles) return;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  __syncthreads();
+  auto tile_bytes = [&](uint64_t tt) {
+    const uint64_t off = tt * kFcBulkTile;
+    return (unsigned)(nbytes - off < kFcBulkTile ? nbytes - off : kFcBulkTile);
+  };
+  if (threadIdx.x == 0) bulk_load(buf[0], src, tile_bytes(t), &mbar[0]);
+  unsigned phase[2] = {0, 0};
+  bool issued = false;
+  for (int b = 0; t < ntiles; t += gridDim.x, b ^= 1) {
+    const uint64_t off = t * kFcBulkTile;
+    const unsigned bytes = tile_bytes(t);
+    /* every thread that stores waits for the tile itself */
+    const bool ready = mbar_wait(&mbar[b], phase[b]);
+    phase[b] ^= 1;
+    if (!ready) {
+      if (threadIdx.x == 0) atomicOr(status, (int)B200SHM_STATUS_TIMEOUT);
+      s_ok = 0;
+    }
+    __syncthreads();
+    if (!s_ok) break;
+    for (int j = threadIdx.x; j < P; j += blockDim.x) {
+      char *d = dst0 + (uint64_t)j * step + (uint64_t)k * nbytes + off;
+      asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(d),
+                   "r"(smem_addr(buf[b])), "r"(bytes)
+                   : "memory");
+      issued = true;
+    }
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    /* the stores of the previous tile (the other buffer) have read it */
+    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0 && t + gridDim.x < ntiles)
+      bulk_load(buf[b ^ 1], src + (t + gridDim.x) * kFcBulkTile, tile_bytes(t + gridDim.x),
+                &mbar[b ^ 1]);
+  }
+  /* this thread's stores complete before the CTA ends */
+  if (issued) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  __syncthreads();
 }
 
 /* collect: member k contributes sizes[k] bytes; member j's
@@ -225,6 +322,16 @@ int fcollect_launch(int pe_start, int pe_stride, int P, uint64_t dest_off, uint6
   Members m = members(pe_start, pe_stride, P);
   const bool vec = ((src_off | dest_off | nbytes | m.step) & 15u) == 0;
   const uint64_t n = vec ? nbytes / 16 : nbytes;
+  static const bool bulk = getenv("B200SHM_FCOLLECT_BULK") && atoi(getenv("B200SHM_FCOLLECT_BULK")) > 0;
+  if (vec && bulk) { /* the staged form, selected for measurement */
+    const uint64_t ntiles = (nbytes + kFcBulkTile - 1) / kFcBulkTile;
+    const uint64_t cap = (8ull * st().sm_count + P - 1) / (uint64_t)P;
+    dim3 g((unsigned)(ntiles < cap ? ntiles : (cap ? cap : 1)), P);
+    k_fcollect_bulk<<<g, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, nbytes,
+                                      st().d_status);
+    count_launch();
+    return B200SHM_OK;
+  }
   dim3 grid(x_blocks(n, P, 8ull * st().sm_count * 4), P);
   if (vec)
     k_fcollect<true><<<grid, 256, 0, s>>>(m.first + src_off, m.first + dest_off, m.step, P, nbytes);

@@ -160,3 +160,39 @@ def test_alltoall_2048_member_world():
                              orc=os.path.join(ROOT, "oracle"), tst=os.path.join(ROOT, "tests"))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+BULK_FCOLLECT = textwrap.dedent("""
+    import sys
+    import numpy as np
+    sys.path[:0] = [{pkg!r}, {orc!r}, {tst!r}]
+    import b200shm as B, gen, oracle
+    rs = oracle.Restatement()
+    B.init(256, 8 << 20)
+    for P, nb in ((1, 16), (2, 48), (8, 8192), (8, 8208), (13, 40960), (128, 32768),
+                  (256, 4096), (64, 100000 // 16 * 16)):
+        x = gen.uniform_int(np.uint8, P, nb, P * 31 + nb)
+        team = (0, 1, P)
+        src, dst = B.malloc(nb), B.malloc(P * nb)
+        B.put_rows(src, x, team=team)
+        B.memset(dst, 0x5A, P * nb, team=team)
+        B.fcollect(dst, src, nb, team=team)
+        got = B.get_rows(dst, P * nb, np.uint8, team=team)
+        assert got.tobytes() == rs.fcollect(x).tobytes(), (P, nb)
+        B.free(src); B.free(dst)
+    B.finalize()
+    print("ok")
+""")
+
+
+def test_fcollect_staged_through_shared_memory():
+    """The fcollect form that stages tiles in shared memory with bulk copies
+    (selected by B200SHM_FCOLLECT_BULK=1): single and multiple tiles, a
+    partial last tile, 1 to 256 members; bit-exact with the oracle."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    code = BULK_FCOLLECT.format(pkg=os.path.join(ROOT, "osss-ucx_b200"),
+                                orc=os.path.join(ROOT, "oracle"), tst=os.path.join(ROOT, "tests"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, B200SHM_FCOLLECT_BULK="1"))
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
