@@ -188,7 +188,8 @@ def run_reference_arm(args, rank):
             "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": kind,
                              "sample": desc},
             "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "config1": config1_cpu_reference()}
     print(json.dumps(line), flush=True)
 
 
@@ -238,6 +239,9 @@ def main():
     ap.add_argument("--batch-reductions", type=int, default=4096)
     ap.add_argument("--batch-tune", default="auto", choices=["auto", "off"],
                     help="batch workload: the autotuner (auto, the default) or the heuristic plan")
+    ap.add_argument("--movement-npes", type=int, default=128,
+                    help="movement workload: PEs (128 is the configuration; 64 keeps profiling "
+                         "captures to a few GB)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the config1/movement/batch/serve sub-objects of the default line")
     args = ap.parse_args()
@@ -418,6 +422,32 @@ def main():
 # ---------------------------------------------------------------------------
 # config 1: 8 PEs, int32 sum reduce + fcollect64 + barrier_all, latency
 # ---------------------------------------------------------------------------
+def config1_cpu_reference(reps=300):
+    """The reference's own shcoll code for config 1 over 8 emulated PEs on
+    the host: median microseconds per call (None without oracle/_ref)."""
+    import gen
+    import oracle
+    if not oracle.Reference.available:
+        return None
+    x, fc = gen.config1_inputs()
+    R = oracle.Reference()
+    out = np.zeros_like(x)
+    _, t_red = R.run(oracle.K_REDUCE_TEAM, "shcoll_int32_sum_reduce_rec_dbl", x, out,
+                     nelems=1024, warmup=20, iters=reps, pin=True)
+    out = np.zeros((8, 8 * 256), np.int64)
+    _, t_fc = R.run(oracle.K_SIZED, "shcoll_fcollect64_bruck_inplace", fc, out, nelems=256,
+                    warmup=20, iters=reps, pin=True)
+    _, t_bar = R.run(oracle.K_BARRIER_ALL, "shcoll_barrier_all_binomial_tree",
+                     np.zeros((8, 8), np.uint8), np.zeros((8, 8), np.uint8), warmup=20,
+                     iters=reps, pin=True)
+    m = [float(np.median(t)) * 1e6 for t in (t_red, t_fc, t_bar)]
+    return {"int32_sum_reduce_us": round(m[0], 2), "fcollect64_us": round(m[1], 2),
+            "barrier_all_us": round(m[2], 2), "sequence_us": round(sum(m), 2),
+            "kind": "reference", "cores": 8,
+            "sample": "the reference's src/shcoll/src code (oracle/_ref) over 8 emulated PEs "
+                      "(pinned pthreads); median of %d calls between host barriers" % reps}
+
+
 def run_config1(args, world, rank, local, reps=300):
     """The reference's CPU-runnable configuration on the GPU: 8 PEs, team
     WORLD, int32 sum_reduce of 1024 elements (rec_dbl, the default), then
@@ -430,7 +460,6 @@ def run_config1(args, world, rank, local, reps=300):
     __graft_entry__.build_library()
     import b200shm as B
     import gen
-    import oracle
     x, fc = gen.config1_inputs()
     B.init(8, 4 << 20)
     team = (0, 1, 8)
@@ -477,24 +506,7 @@ def run_config1(args, world, rank, local, reps=300):
                  z["fcollect_out"].tobytes())
     finally:
         B.finalize()
-    cpu = None
-    if oracle.Reference.available:
-        R = oracle.Reference()
-        out = np.zeros_like(x)
-        _, t_red = R.run(oracle.K_REDUCE_TEAM, "shcoll_int32_sum_reduce_rec_dbl", x, out,
-                         nelems=1024, warmup=20, iters=reps, pin=True)
-        out = np.zeros((8, 8 * 256), np.int64)
-        _, t_fc = R.run(oracle.K_SIZED, "shcoll_fcollect64_bruck_inplace", fc, out, nelems=256,
-                        warmup=20, iters=reps, pin=True)
-        _, t_bar = R.run(oracle.K_BARRIER_ALL, "shcoll_barrier_all_binomial_tree",
-                         np.zeros((8, 8), np.uint8), np.zeros((8, 8), np.uint8), warmup=20,
-                         iters=reps, pin=True)
-        m = [float(np.median(t)) * 1e6 for t in (t_red, t_fc, t_bar)]
-        cpu = {"int32_sum_reduce_us": round(m[0], 2), "fcollect64_us": round(m[1], 2),
-               "barrier_all_us": round(m[2], 2), "sequence_us": round(sum(m), 2),
-               "kind": "reference", "cores": 8,
-               "sample": "the reference's src/shcoll/src code (oracle/_ref) over 8 emulated PEs "
-                         "(pinned pthreads); median of %d calls between host barriers" % reps}
+    cpu = config1_cpu_reference(reps)
     return {"workload": "config1: 8 PEs, int32 sum_reduce 1024 + fcollect64 256 + barrier_all",
             "unit": "us per call (median of %d)" % reps, "gpu": gpu, "cpu_reference": cpu,
             "bit_exact_vs_golden": bool(exact)}
@@ -549,8 +561,10 @@ def run_movement(args, world, rank, local):
     import gen
     import oracle
     rs = oracle.Restatement()
-    PM, BLK, NS, NF, NOPS, NCNT = 128, 64 << 10, 4096, 4096, 1 << 20, 1 << 20
-    B.init(PM, 96 << 20)  # 12 GiB arena: 76 MiB of objects per PE
+    PM, BLK, NS, NF, NOPS, NCNT = args.movement_npes, 64 << 10, 4096, 4096, 1 << 20, 1 << 20
+    # 128 PEs (the configuration): 12 GiB arena, 76 MiB of objects per PE;
+    # fewer PEs (profiling captures): the same per-pair sizes in a smaller arena
+    B.init(PM, (96 if PM > 64 else 64) << 20)
     team = (0, 1, PM)
     s_ptr = B.stream()
     st = torch.cuda.ExternalStream(s_ptr)
@@ -638,7 +652,7 @@ def run_movement(args, world, rank, local):
     ok = ok and np.array_equal(fs, (runs - 1) * hist[ks] + rank_in)
     res["atomic_fetch_add"]["bit_exact"] = bool(ok)
     B.finalize()
-    cpu = movement_cpu_reference()
+    cpu = movement_cpu_reference() if PM == 128 and not args.no_cpu_baseline else None
     return {"workload": "movement", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "peak_gbs": peak, "peak_kind": peak_kind,
             "config": {"npes": PM, "alltoallmem_block": BLK, "alltoalls": "int64 dst=2 sst=3 n=4096",

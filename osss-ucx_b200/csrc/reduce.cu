@@ -907,13 +907,24 @@ extern "C" int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, voi
     return fail(B200SHM_ERR_ARG, "reduce_noalloc: buffer span wraps the address space");
   /* The kernels read every member's source row of a column while other
    * CTAs write dest rows, and the float MIN/MAX replay reads the sources
-   * after the dests of other elements are written: so the dest rows and the
-   * source rows must be either the very same rows (in place: same base,
-   * same stride) or fully apart. */
+   * after the dests of other elements are written: so no dest row may
+   * touch any source row, except that a dest row may be its own member's
+   * source row (in place: same base, same stride).  Source rows are
+   * disjoint and sorted (stride >= row size), so a dest row can only touch
+   * the source row at or before its start and the one after: O(npes). */
   const bool in_place = d0 == s0 && (dest_stride == source_stride || npes == 1);
-  if (!in_place && overlaps(d0, dspan, s0, sspan))
-    return fail(B200SHM_ERR_ARG,
-                "reduce_noalloc: dest rows and source rows overlap without being the same rows");
+  for (uint64_t i = 0; i < (uint64_t)npes; i++) {
+    const uint64_t di = d0 + i * dest_stride;
+    uint64_t jc = 0;
+    if (npes > 1 && di >= s0) jc = (di - s0) / source_stride;
+    for (uint64_t j = jc; j <= jc + 1 && j < (uint64_t)npes; j++) {
+      if (in_place && j == i) continue;
+      if (overlaps(di, bytes, s0 + j * source_stride, bytes))
+        return fail(B200SHM_ERR_ARG,
+                    "reduce_noalloc: member %llu's dest row overlaps member %llu's source row",
+                    (unsigned long long)i, (unsigned long long)j);
+    }
+  }
   const bool minmax_float = (op == B200SHM_MIN || op == B200SHM_MAX) &&
                             (dtype == B200SHM_F32 || dtype == B200SHM_F64);
   if (minmax_float && nelems > kNoAllocMaxDeferred)

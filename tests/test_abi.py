@@ -76,3 +76,28 @@ def test_every_openshmem_declaration_is_exported():
             except AttributeError:
                 missing.append((h, name))
     assert not missing, missing[:20]
+
+
+def test_noalloc_row_overlap_rules_without_a_gpu():
+    """b200shm_reduce_noalloc checks its rows before it touches the device:
+    interleaved rows (dest and source rows of different offsets in the same
+    slices) and in-place rows pass the checks, any dest row that touches
+    another member's source row is refused.  Without a GPU a call that
+    passes the checks stops at the device (a CUDA error), so the code tells
+    which way the check went.  Skipped where a GPU is present, since there
+    a call that passes would run on these made-up addresses."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    L = b200shm.lib
+    base, sb, n = 1 << 40, 1 << 20, 256  # int32 rows of 1 KiB in slices of 1 MiB
+
+    def call(dst, ds, src, ss, P=4):
+        return L.b200shm_reduce_noalloc(5, 2, 2, P, dst, ds, src, ss, n, None)
+    assert call(base + 4096, sb, base, sb) == -4          # interleaved: checks pass
+    assert call(base, sb, base, sb) == -4                 # in place: checks pass
+    assert call(base + 8 * sb, 2 * sb, base, sb) == -4    # apart, other stride
+    for dst, ds, src, ss in [(base + sb + 4, sb, base, sb), (base, sb, base, 2 * sb),
+                             (base + 64, sb, base, sb), (base + 3 * sb - 512, sb, base, sb)]:
+        assert call(dst, ds, src, ss) == -1, (dst - base, ds, ss)
+        assert b"overlaps" in L.b200shm_last_error()
