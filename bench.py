@@ -402,7 +402,12 @@ def main():
         for name, fn in (("config1", run_config1), ("movement", run_movement),
                          ("batch", run_batch), ("serve", run_serve)):
             t0 = time.perf_counter()
-            extras[name] = fn(args, world, rank, local)
+            try:
+                extras[name] = fn(args, world, rank, local)
+            except Exception as e:  # the headline line is printed whatever happens here
+                extras[name] = {"error": "%s: %s" % (type(e).__name__, e)}
+                if B.initialized():
+                    B.finalize()
             extras[name]["run_seconds"] = round(time.perf_counter() - t0, 1)
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),

@@ -431,6 +431,8 @@ def replay(reqs, arrival_s, server=None):
 def replay_ordered(reqs, stream=None):
     """Every request through its per-call entry point, stream-ordered, one
     synchronisation at the end: returns (seconds, fetched values)."""
+    if not isinstance(reqs, ctypes.Array):  # e.g. a slice of an array: a list of requests
+        reqs = (Request * len(reqs))(*reqs)
     n = len(reqs)
     fet = np.zeros(n, np.uint64)
     sec = ctypes.c_double()

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) k_fcollect_bulk(const char *src0, char *d
     const uint64_t off = tt * kFcBulkTile;
     return (unsigned)(nbytes - off < kFcBulkTile ? nbytes - off : kFcBulkTile);
   };
-  if (threadIdx.x == 0) bulk_load(buf[0], src, tile_bytes(t), &mbar[0]);
+  if (threadIdx.x == 0) bulk_load(buf[0], src + t * kFcBulkTile, tile_bytes(t), &mbar[0]);
   unsigned phase[2] = {0, 0};
   bool issued = false;
   for (int b = 0; t < ntiles; t += gridDim.x, b ^= 1) {

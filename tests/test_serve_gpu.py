@@ -342,3 +342,25 @@ def test_wait_on_a_ticket_that_never_completes_times_out(B, heap):
     finally:
         srv.stop()
     assert B.get_rows(a, 8, np.int64, team=(0, 1, 1))[0, 0] == 6
+
+
+def test_stream_ordered_per_call_matches_blocking(B, heap, src_region):
+    """b200shm_serve_replay_ordered (every request's per-call entry point
+    back to back on one stream) leaves what the blocking per-call replay
+    leaves, and hands back AMO old values as a permutation."""
+    rng = np.random.default_rng(12)
+    dests, items = [], []
+    for kind in ["reduce"] * 12 + ["fcollect", "alltoall", "put", "get"] * 3:
+        items.append(random_request(rng, src_region, dests, heap, kinds=[kind]))
+    ctr = heap(8)
+    B.memset(ctr, 0, 8, team=(5, 1, 1))
+    items += [dict(kind="amo", op="fetch_add", dtype="int64", pe=5, dest=ctr, value=1)] * 16
+    reqs = B.make_requests(items)
+    B.replay(reqs, np.zeros(len(items)))
+    want = read_dests(B, dests)
+    clear_dests(B, dests)
+    B.memset(ctr, 0, 8, team=(5, 1, 1))
+    sec, fetched = B.replay_ordered(reqs[:])  # a slice: a list of requests
+    assert sec > 0
+    assert read_dests(B, dests) == want
+    assert sorted(fetched[-16:].tolist()) == list(range(16))
