@@ -11,6 +11,7 @@ import socket
 import sys
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -133,3 +134,35 @@ def test_three_ranks_fold_in_rank_order():
 
 def test_four_ranks():
     check(4)
+
+
+@pytest.mark.gpu
+def test_engine_steps_on_one_gpu(B, heap, rs):
+    """The engine-backed steps on the GPU, in a world of one rank: the local
+    partial is the engine's reduction over the local members, viewed in
+    place as a tensor, and the write-back broadcasts it to every local
+    member -- the same bits as b200shm_reduce over those members."""
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "osss-ucx_b200"))
+    import gen
+    import spanning
+    port = free_port()
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                            world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        for op, dtype, algo, P in (("sum", "float32", "rec_dbl", 8), ("xor", "int64", "linear", 5),
+                                   ("max", "float64", "rabenseifner", 16)):
+            x = inputs(op, dtype, P, P)
+            src, dst = heap(x[0].nbytes), heap(x[0].nbytes)
+            team = (10, 3, P)
+            B.put_rows(src, x, team=team)
+            B.memset(dst, 0x5A, x[0].nbytes, team=team)
+            t = spanning.SpanningTeam(B, P, local_start=10, local_stride=3)
+            assert t.reduce(op, dtype, algo, dst, src, N)
+            got = B.get_rows(dst, x[0].nbytes, x.dtype, team=team)
+            want = rs.reduce(algo, op, x)
+            assert (got == want[0]).all() and got.tobytes() == np.broadcast_to(
+                want[0], want.shape).tobytes(), (op, dtype, algo)
+    finally:
+        dist.destroy_process_group()
