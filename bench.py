@@ -457,10 +457,11 @@ def run_config1(args, world, rank, local, reps=300):
     """The reference's CPU-runnable configuration on the GPU: 8 PEs, team
     WORLD, int32 sum_reduce of 1024 elements (rec_dbl, the default), then
     fcollect64 of 256 int64 per PE, then barrier_all (binomial tree).  These
-    are latency-bound; reported in microseconds per call: blocking calls
-    through the C ABI (launch + synchronisation each, what an OpenSHMEM
-    call costs) and the three stream-ordered with one synchronisation; next
-    to the reference's own shcoll code over 8 emulated PEs on the host."""
+    are latency-bound; reported in microseconds per call, timed on the host
+    around the C entry points: blocking calls (launch + synchronisation
+    each, what an OpenSHMEM call costs) and the three stream-ordered with
+    one synchronisation; next to the reference's own shcoll code over 8
+    emulated PEs on the host."""
     import __graft_entry__
     __graft_entry__.build_library()
     import b200shm as B
@@ -475,14 +476,24 @@ def run_config1(args, world, rank, local, reps=300):
         B.put_rows(fs, fc, team=team)
         s_ptr = B.stream()
 
+        # the C entry points called directly (arguments converted once), so
+        # the figures are the engine's per-call cost, not the binding's
+        L = B.lib
+        r_args = (B.OPS.index("sum"), B.DTYPES.index("int32"), B.ALGOS.index("rec_dbl"), 0, 1, 8,
+                  dst, src, 1024)
+        bar_algo = B.BARRIER_ALGOS.index("binomial_tree")
+
         def red(stream=None):
-            B.reduce("sum", "int32", "rec_dbl", dst, src, 1024, team=team, stream=stream)
+            if L.b200shm_reduce(*r_args, stream):
+                raise B.B200Error(-1, L.b200shm_last_error().decode())
 
         def fcol(stream=None):
-            B.fcollect(fd, fs, 2048, team=team, stream=stream)
+            if L.b200shm_fcollect(0, 1, 8, fd, fs, 2048, stream):
+                raise B.B200Error(-1, L.b200shm_last_error().decode())
 
         def bar(stream=None):
-            B.barrier("binomial_tree", team=team, stream=stream)
+            if L.b200shm_barrier(bar_algo, 0, 1, 8, stream):
+                raise B.B200Error(-1, L.b200shm_last_error().decode())
 
         def seq():
             red(), fcol(), bar()

@@ -495,7 +495,7 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
        * so G = 2 at 64 leaves; chains: G = 2 */
       int G = 2;
       if constexpr (ORDER != ORD_CHAIN) G = std::max(2, std::min(8, nleaves / 32));
-      const char *ec = getenv("B200SHM_REDUCE_COOP");
+      static const char *ec = getenv("B200SHM_REDUCE_COOP"); /* read once */
       if (ec) G = atoi(ec);
       if (G < 1) G = 1;
       if (G > 32) G = 32;

@@ -1,8 +1,9 @@
 /*
  * sync.cu -- device barriers among the members of a team.
  *
- * Each member is one PE context (a thread) of a cooperative launch, so all
- * contexts are resident together.  They synchronise through flag words
+ * Each member is one PE context (a thread); the contexts of a team of more
+ * than 256 members are the CTAs of a cooperative launch, so all of them
+ * are resident together (a team of up to 256 is one CTA, which always is).  They synchronise through flag words
  * with the message pattern of the reference algorithm chosen
  * (src/shcoll/src/barrier.c): poke = atomic add with release semantics
  * (shmem_long_atomic_inc), wait = acquire load loop (shmem_long_wait_until,
@@ -205,8 +206,18 @@ int barrier_launch(int algo, int pe_start, int pe_stride, int P, cudaStream_t s,
   a.absent = absent;
   const int threads = P < 256 ? P : 256;
   const int blocks = (P + threads - 1) / threads;
-  int per_sm = 0;
-  B200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier, threads, 0));
+  if (blocks == 1) { /* one CTA is always resident as a whole: a plain launch */
+    k_barrier<<<1, threads, 0, s>>>(a);
+    count_launch();
+    return B200SHM_OK;
+  }
+  /* CTAs of 256 contexts one SM holds at once (queried once) */
+  static std::atomic<int> per_sm_cache{0};
+  int per_sm = per_sm_cache.load(std::memory_order_relaxed);
+  if (per_sm == 0) {
+    B200_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier, 256, 0));
+    per_sm_cache.store(per_sm, std::memory_order_relaxed);
+  }
   if ((long long)per_sm * st().sm_count < blocks)
     return fail(B200SHM_ERR_UNSUPPORTED, "barrier: %d PE contexts cannot be co-resident", P);
   void *args[] = {(void *)&a};
