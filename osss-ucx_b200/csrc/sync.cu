@@ -3,7 +3,8 @@
  *
  * Each member is one PE context (a thread); the contexts of a team of more
  * than 256 members are the CTAs of a cooperative launch, so all of them
- * are resident together (a team of up to 256 is one CTA, which always is).  They synchronise through flag words
+ * are resident together (a team of up to 256 is one CTA, which always is,
+ * and keeps its flag words in shared memory).  They synchronise through flag words
  * with the message pattern of the reference algorithm chosen
  * (src/shcoll/src/barrier.c): poke = atomic add with release semantics
  * (shmem_long_atomic_inc), wait = acquire load loop (shmem_long_wait_until,
@@ -40,7 +41,16 @@ struct BArgs {
   int absent;      /* member that never arrives (failure injection), or -1 */
 };
 
-__device__ __forceinline__ unsigned long long *flag(const BArgs &a, int member, int round) {
+/* Flag words: for a team over several CTAs, one 64-byte line per (global
+ * PE, round) in the library's global area, used with gpu-scope
+ * release/acquire; for a team that is one CTA (up to 256 members), the
+ * same pattern on words in that CTA's shared memory with cta scope, which
+ * costs tens of nanoseconds a hop instead of a round trip to L2. */
+constexpr int kCtaRounds = 8; /* dissemination rounds of a 256-member team */
+template <bool CTA>
+__device__ __forceinline__ unsigned long long *flag(const BArgs &a, unsigned long long *sfl,
+                                                   int member, int round) {
+  if constexpr (CTA) return sfl + member * kCtaRounds + round;
   const uint64_t pe = (uint64_t)a.pe_start + (uint64_t)member * (uint64_t)a.pe_stride;
   return a.flags + (pe * (uint64_t)a.rounds + (uint64_t)round) * 8ull;
 }
@@ -49,30 +59,37 @@ __device__ __forceinline__ long long now_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+template <bool CTA>
 __device__ __forceinline__ unsigned long long ld_acq(const unsigned long long *p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  if constexpr (CTA) asm volatile("ld.acquire.cta.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  else asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+template <bool CTA>
 __device__ __forceinline__ void poke(unsigned long long *p, unsigned long long v = 1) {
-  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+  if constexpr (CTA) asm volatile("red.release.cta.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+  else asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+template <bool CTA>
 __device__ __forceinline__ void st_rel(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+  if constexpr (CTA) asm volatile("st.release.cta.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+  else asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 enum { W_EQ, W_NE, W_GE };
 /* Bounded wait; false (and the TIMEOUT bit) when the budget runs out. */
+template <bool CTA>
 __device__ bool wait_flag(const BArgs &a, unsigned long long *p, int cmp, unsigned long long v,
                           long long deadline) {
   for (;;) {
-    const unsigned long long x = ld_acq(p);
+    const unsigned long long x = ld_acq<CTA>(p);
     if (cmp == W_EQ ? x == v : cmp == W_NE ? x != v : x >= v) return true;
     if (now_ns() > deadline) {
       atomicOr(a.status, (int)B200SHM_STATUS_TIMEOUT);
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(CTA ? 32 : 64);
   }
 }
 
@@ -119,64 +136,84 @@ __device__ int knomial_node(int i, int n, int k, int *parent, int *ch) {
 }
 
 /* gather-to-root then release, barrier.c:96-228 */
-__device__ void tree_barrier(const BArgs &a, int me, int parent, const int *ch, int nch,
-                             long long deadline) {
-  unsigned long long *mine = flag(a, me, 0);
-  if (nch && !wait_flag(a, mine, W_EQ, (unsigned long long)nch, deadline)) return;
+template <bool CTA>
+__device__ void tree_barrier(const BArgs &a, unsigned long long *sfl, int me, int parent,
+                             const int *ch, int nch, long long deadline) {
+  unsigned long long *mine = flag<CTA>(a, sfl, me, 0);
+  if (nch && !wait_flag<CTA>(a, mine, W_EQ, (unsigned long long)nch, deadline)) return;
   if (parent >= 0) {
-    poke(flag(a, parent, 0));
-    if (!wait_flag(a, mine, W_EQ, (unsigned long long)nch + 1, deadline)) return;
+    poke<CTA>(flag<CTA>(a, sfl, parent, 0));
+    if (!wait_flag<CTA>(a, mine, W_EQ, (unsigned long long)nch + 1, deadline)) return;
   }
-  st_rel(mine, 0);
-  for (int c = 0; c < nch; c++) poke(flag(a, ch[c], 0));
+  st_rel<CTA>(mine, 0);
+  for (int c = 0; c < nch; c++) poke<CTA>(flag<CTA>(a, sfl, ch[c], 0));
 }
 
-__global__ void k_barrier(const BArgs a) {
-  const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= a.P || me == a.absent) return;
+/* One PE context's part of barrier a.algo (member `me`). */
+template <bool CTA>
+__device__ void barrier_body(const BArgs &a, unsigned long long *sfl, int me) {
   const long long deadline = now_ns() + a.budget_ns;
   const int P = a.P;
   int ch[32];
   switch (a.algo) {
   case B200SHM_BAR_LINEAR: { /* barrier.c:56-84 */
-    unsigned long long *mine = flag(a, me, 0);
+    unsigned long long *mine = flag<CTA>(a, sfl, me, 0);
     if (me == 0) {
-      if (!wait_flag(a, mine, W_EQ, (unsigned long long)(P - 1), deadline)) return;
-      st_rel(mine, 0);
-      for (int i = 1; i < P; i++) st_rel(flag(a, i, 0), 1);
+      if (!wait_flag<CTA>(a, mine, W_EQ, (unsigned long long)(P - 1), deadline)) return;
+      st_rel<CTA>(mine, 0);
+      for (int i = 1; i < P; i++) st_rel<CTA>(flag<CTA>(a, sfl, i, 0), 1);
     } else {
-      poke(flag(a, 0, 0));
-      if (!wait_flag(a, mine, W_NE, 0, deadline)) return;
-      st_rel(mine, 0);
+      poke<CTA>(flag<CTA>(a, sfl, 0, 0));
+      if (!wait_flag<CTA>(a, mine, W_NE, 0, deadline)) return;
+      st_rel<CTA>(mine, 0);
     }
     break;
   }
   case B200SHM_BAR_COMPLETE_TREE: { /* barrier.c:96-132, degree 2 */
     const int n = complete_children(me, P, 2, ch);
-    tree_barrier(a, me, me ? (me - 1) / 2 : -1, ch, n, deadline);
+    tree_barrier<CTA>(a, sfl, me, me ? (me - 1) / 2 : -1, ch, n, deadline);
     break;
   }
   case B200SHM_BAR_BINOMIAL_TREE: { /* barrier.c:144-180 */
     const int n = binomial_children(me, P, ch);
-    tree_barrier(a, me, me ? (me & (me - 1)) : -1, ch, n, deadline);
+    tree_barrier<CTA>(a, sfl, me, me ? (me & (me - 1)) : -1, ch, n, deadline);
     break;
   }
   case B200SHM_BAR_KNOMIAL_TREE: { /* barrier.c:192-228, radix 2 */
     int parent;
     const int n = knomial_node(me, P, 2, &parent, ch);
-    tree_barrier(a, me, parent, ch, n, deadline);
+    tree_barrier<CTA>(a, sfl, me, parent, ch, n, deadline);
     break;
   }
   default: { /* dissemination, barrier.c:241-266 */
     for (int r = 0, d = 1; d < P; r++, d <<= 1) {
-      poke(flag(a, (me + d) % P, r));
-      unsigned long long *mine = flag(a, me, r);
-      if (!wait_flag(a, mine, W_NE, 0, deadline)) return;
+      poke<CTA>(flag<CTA>(a, sfl, (me + d) % P, r));
+      unsigned long long *mine = flag<CTA>(a, sfl, me, r);
+      if (!wait_flag<CTA>(a, mine, W_NE, 0, deadline)) return;
       atomicAdd(mine, (unsigned long long)-1ll);
     }
     break;
   }
   }
+}
+
+/* a team over several CTAs (cooperative launch), flags in global memory */
+__global__ void k_barrier(const BArgs a) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= a.P || me == a.absent) return;
+  barrier_body<false>(a, nullptr, me);
+}
+
+/* a team of up to 256 members as one CTA, flags in its shared memory
+ * (zeroed before any context pokes one; the contexts that do not take
+ * part leave only after that) */
+__global__ void __launch_bounds__(256) k_barrier_cta(const BArgs a) {
+  __shared__ unsigned long long sfl[256 * kCtaRounds];
+  for (int i = threadIdx.x; i < 256 * kCtaRounds; i += blockDim.x) sfl[i] = 0;
+  __syncthreads();
+  const int me = threadIdx.x;
+  if (me >= a.P || me == a.absent) return;
+  barrier_body<true>(a, sfl, me);
 }
 
 }  // namespace
@@ -206,8 +243,8 @@ int barrier_launch(int algo, int pe_start, int pe_stride, int P, cudaStream_t s,
   a.absent = absent;
   const int threads = P < 256 ? P : 256;
   const int blocks = (P + threads - 1) / threads;
-  if (blocks == 1) { /* one CTA is always resident as a whole: a plain launch */
-    k_barrier<<<1, threads, 0, s>>>(a);
+  if (blocks == 1) { /* one CTA, flags in its shared memory: a plain launch */
+    k_barrier_cta<<<1, threads, 0, s>>>(a);
     count_launch();
     return B200SHM_OK;
   }

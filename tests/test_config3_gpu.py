@@ -146,6 +146,11 @@ WORLD_2048 = textwrap.dedent("""
     B.alltoalls(dst, src, 2, 3, n, 8, team=team)
     got = B.get_rows(dst, d0[0].nbytes, np.int64, team=team)
     assert got.tobytes() == rs.alltoalls(x, d0, 2, 3, n).tobytes(), "alltoalls"
+    # barriers over more members than one CTA holds: the cooperative form
+    for algo in B.BARRIER_ALGOS:
+        for tm in ((0, 1, 2048), (5, 3, 300), (0, 1, 257)):
+            for _ in range(2):
+                B.barrier(algo, team=tm)
     B.finalize()
     print("ok")
 """)
@@ -153,7 +158,8 @@ WORLD_2048 = textwrap.dedent("""
 
 def test_alltoall_2048_member_world():
     """The 2048-PE world of the batching configuration: shmem_alltoallmem /
-    alltoalls64 on every PE at once (4M pairs), in a process of its own."""
+    alltoalls64 on every PE at once (4M pairs), and barriers over 257-2048
+    members (several CTAs, a cooperative launch), in a process of its own."""
     import __graft_entry__
     __graft_entry__.build_library()
     code = WORLD_2048.format(pkg=os.path.join(ROOT, "osss-ucx_b200"),
