@@ -29,6 +29,14 @@ P * eps * sum|x| of the exact sum, the bound of the reference's own
 arrival-order binomial reduction.  Ranks that are not a power of two
 combine the partials by an all-gather and a left fold in rank order.
 
+The data movement follows the same split: fcollect gathers the local
+members' blocks with the engine and all-gathers the local concatenation
+across ranks; alltoall moves the blocks between local members with the
+engine and the rest in one all-to-all across ranks; atomics are routed to
+the rank that owns their target member and run there as one batch, their
+old values returned in the caller's order.  All three are byte-exact for
+any team.
+
 Step 2 moves N elements per round over NCCL (point-to-point over NVLink);
 no TMA multicast is used anywhere on this path.  Nothing here has run on
 more than one GPU: this pool gives one GPU per job, so the cross-rank
@@ -157,6 +165,121 @@ class SpanningTeam:
         result = butterfly_allreduce(partial.clone(), op, self.group)
         self.write_back(result, dest, nelems, dtype)
         return self.exact(op, dtype, algo)
+
+    # -- data movement (byte-exact for any team) -------------------------------
+    def row(self, i, off, nbytes):
+        """Local member i's `nbytes` at offset `off`, as a uint8 tensor view."""
+        start, stride, _ = self.local
+        return _device_tensor(self.B.ptr(start + i * stride, off), nbytes, "uint8")
+
+    def local_fcollect(self, dest, src, nbytes):
+        """The local members' blocks in their global places of every local
+        member's dest: the engine's fcollect over the local team."""
+        start, stride, size = self.local
+        self.B.fcollect(dest + self.rank * size * nbytes, src, nbytes, team=(start, stride, size))
+
+    def local_alltoall(self, dest, src, nbytes):
+        """The blocks between local members: the engine's alltoall over the
+        local team on the local part of the block index."""
+        start, stride, size = self.local
+        o = self.rank * size * nbytes
+        self.B.alltoall(dest + o, src + o, nbytes, team=(start, stride, size))
+
+    def sync_device(self):
+        torch.cuda.synchronize()
+
+    def fcollect(self, dest, src, nbytes):
+        """Every member's dest holds the P members' blocks in member order
+        (fcollect_helper_*, src/shcoll/src/fcollect.c:32-484): the local
+        members' blocks by the engine, then one all-gather of the local
+        concatenation across ranks, written into every local member."""
+        L = self.local[2]
+        self.local_fcollect(dest, src, nbytes)
+        self.sync_device()
+        mine = self.row(0, dest + self.rank * L * nbytes, L * nbytes).clone()
+        parts = [torch.empty_like(mine) for _ in range(self.world)]
+        dist.all_gather(parts, mine, group=self.group)
+        for i in range(L):
+            d = self.row(i, dest, self.world * L * nbytes)
+            for r, part in enumerate(parts):
+                if r != self.rank:
+                    d[r * L * nbytes:(r + 1) * L * nbytes].copy_(part)
+        self.sync_device()
+
+    def alltoall(self, dest, src, nbytes):
+        """Member j's dest block k = member k's source block j
+        (alltoall_helper_*, src/shcoll/src/alltoall.c:75-201): the blocks
+        between local members by the engine, the rest in one all-to-all
+        across ranks (rank r sends rank q the L x L blocks its members hold
+        for q's members)."""
+        L, G, r, B = self.local[2], self.world, self.rank, nbytes
+        self.local_alltoall(dest, src, nbytes)
+        self.sync_device()
+        srows = [self.row(i, src, G * L * B) for i in range(L)]
+        # send[q] = [my member k][q's member j] blocks (q == r: unused)
+        send = torch.stack([torch.stack([srows[i][q * L * B:(q + 1) * L * B] for i in range(L)])
+                            for q in range(G)]).reshape(-1)
+        recv = torch.empty_like(send)
+        dist.all_to_all_single(recv, send, group=self.group)
+        recv = recv.view(G, L, L, B)  # [sender rank q][its member k][my member j]
+        drows = [self.row(j, dest, G * L * B) for j in range(L)]
+        for q in range(G):
+            if q == r:
+                continue
+            blk = recv[q]
+            for j in range(L):
+                drows[j][q * L * B:(q + 1) * L * B].copy_(blk[:, j, :].reshape(-1))
+        self.sync_device()
+
+    # -- atomics routed to the rank that owns the target ----------------------
+    def local_amo(self, amo, dtype, pe_local, off, value):
+        """Run a batch of atomics on this rank's members (the engine's
+        b200shm_amo_batch, 8-byte operands); returns the old values (int64,
+        on the CPU)."""
+        start, stride, _ = self.local
+        n = len(pe_local)
+        if n == 0:
+            return torch.zeros(0, dtype=torch.int64)
+        pe = (start + pe_local.to(torch.int64) * stride).to(torch.int32).cuda()
+        o = off.to(torch.int64).cuda()  # byte offsets, read by the engine as uint64
+        v = value.to(torch.int64).cuda()
+        f = torch.zeros(n, dtype=torch.int64, device="cuda")
+        self.B.amo_batch(amo, dtype, n, pe.data_ptr(), o.data_ptr(), v.data_ptr(), None,
+                         f.data_ptr())
+        return f.cpu()
+
+    def amo(self, amo, dtype, pe, off, value):
+        """Atomics on (member, offset) targets anywhere in the team: each op
+        goes to the rank that owns its member (member // members_per_rank),
+        which runs its share as one batch; the old values come back in the
+        caller's order.  Ops on one word from different ranks are applied in
+        an unspecified order, as concurrent AMOs from different PEs are in
+        OpenSHMEM (src/shmemc/ucx/comms.c:409-671)."""
+        L, G = self.local[2], self.world
+        # the exchanges run where the group's backend wants its tensors
+        dev = "cuda" if dist.get_backend(self.group) == "nccl" else "cpu"
+        pe = torch.as_tensor(pe, dtype=torch.int64)
+        off = torch.as_tensor(off, dtype=torch.int64)
+        value = torch.as_tensor(value, dtype=torch.int64)
+        owner = pe // L
+        order = torch.argsort(owner, stable=True)
+        send_counts = torch.bincount(owner, minlength=G).to(dev)
+        recv_counts = torch.empty_like(send_counts)
+        dist.all_to_all_single(recv_counts, send_counts, group=self.group)
+        sc, rc = send_counts.tolist(), recv_counts.tolist()
+        packed = torch.stack([pe[order] % L, off[order], value[order]], dim=1).to(dev)
+        incoming = torch.empty((sum(rc), 3), dtype=torch.int64, device=dev)
+        dist.all_to_all_single(incoming, packed, output_split_sizes=rc, input_split_sizes=sc,
+                               group=self.group)
+        incoming = incoming.cpu()
+        fetched_here = self.local_amo(amo, dtype, incoming[:, 0], incoming[:, 1],
+                                      incoming[:, 2]).to(dev)
+        back = torch.empty(len(pe), dtype=torch.int64, device=dev)
+        dist.all_to_all_single(back, fetched_here, output_split_sizes=sc, input_split_sizes=rc,
+                               group=self.group)
+        out = torch.empty(len(pe), dtype=torch.int64)
+        out[order] = back.cpu()
+        return out
 
 
 _TORCH = {"int8": torch.int8, "int16": torch.int16, "int32": torch.int32, "int64": torch.int64,
