@@ -224,8 +224,11 @@ __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
  * grow with the tree depth, and a pack's 2*P memory operations are spread
  * over G lanes. */
 
+/* The MIN/MAX-checking instances are held to 64 registers (4 CTAs per
+ * SM; unbounded they take 78 and 3 CTAs), which ptxas meets without
+ * spilling; the others stay at 48 on their own. */
 template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL, bool POW2>
-__global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
+__global__ void __launch_bounds__(256, MM ? 4 : 1) k_reduce_coop(const RArgs a) {
   typedef Pack<T, V> PK;
   constexpr int COLS = 32 / G; /* packs per warp per iteration */
   const int lane = threadIdx.x & 31;
