@@ -224,11 +224,12 @@ __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
  * grow with the tree depth, and a pack's 2*P memory operations are spread
  * over G lanes. */
 
-/* The MIN/MAX-checking instances are held to 64 registers (4 CTAs per
- * SM; unbounded they take 78 and 3 CTAs), which ptxas meets without
- * spilling; the others stay at 48 on their own. */
+/* The MIN/MAX-checking instances take 78 registers (3 CTAs per SM), the
+ * others 48 (5).  Holding the MIN/MAX ones to 64 (4 CTAs per SM, no spills)
+ * measured slower on the 64-PE headline (f64 MAX 5908-5912 against
+ * 5938-5950 GB/s), so they are left unbounded. */
 template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL, bool POW2>
-__global__ void __launch_bounds__(256, MM ? 4 : 1) k_reduce_coop(const RArgs a) {
+__global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
   typedef Pack<T, V> PK;
   constexpr int COLS = 32 / G; /* packs per warp per iteration */
   const int lane = threadIdx.x & 31;
