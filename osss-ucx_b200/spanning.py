@@ -261,6 +261,8 @@ class SpanningTeam:
         pe = torch.as_tensor(pe, dtype=torch.int64)
         off = torch.as_tensor(off, dtype=torch.int64)
         value = torch.as_tensor(value, dtype=torch.int64)
+        if len(pe) and (int(pe.min()) < 0 or int(pe.max()) >= self.size):
+            raise ValueError("amo: target member outside the team of %d" % self.size)
         owner = pe // L
         order = torch.argsort(owner, stable=True)
         send_counts = torch.bincount(owner, minlength=G).to(dev)
