@@ -261,8 +261,13 @@ class SpanningTeam:
         pe = torch.as_tensor(pe, dtype=torch.int64)
         off = torch.as_tensor(off, dtype=torch.int64)
         value = torch.as_tensor(value, dtype=torch.int64)
-        if len(pe) and (int(pe.min()) < 0 or int(pe.max()) >= self.size):
-            raise ValueError("amo: target member outside the team of %d" % self.size)
+        # every rank learns whether any rank has a bad target, so all of them
+        # refuse together instead of leaving the others in the exchange
+        bad = torch.tensor([int(len(pe) > 0 and (int(pe.min()) < 0 or
+                                                 int(pe.max()) >= self.size))], device=dev)
+        dist.all_reduce(bad, op=dist.ReduceOp.MAX, group=self.group)
+        if int(bad.item()):
+            raise ValueError("amo: a target member outside the team of %d" % self.size)
         owner = pe // L
         order = torch.argsort(owner, stable=True)
         send_counts = torch.bincount(owner, minlength=G).to(dev)
