@@ -279,6 +279,15 @@ def _movement_rank_main(rank, world, port, q):
                 seen.setdefault((m, c), []).append(f)
         ok_p = all(sorted(v) == list(range(len(v))) for v in seen.values())
         res.append((L, nb, ok_f, ok_a, bool(ok_c), ok_p))
+    # one rank names a member outside the team: every rank refuses the call
+    t = CpuArena(2, 1 << 12, 8)
+    bad_pe = np.array([2 * world if rank == 0 else 0])
+    try:
+        t.amo("fetch_add", "int64", bad_pe, np.zeros(1, np.int64), np.ones(1, np.int64))
+        refused = False
+    except ValueError:
+        refused = True
+    res.append((0, 0, refused, refused, refused, refused))
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, res))
