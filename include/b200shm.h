@@ -235,6 +235,52 @@ int b200shm_barrier_absent(int algo, int pe_start, int pe_stride, int pe_size, i
 int64_t b200shm_barrier_flags_nonzero(void);
 
 /* ---------------------------------------------------------------------- */
+/* teams that span GPUs (one process and one engine per GPU)               */
+/* ---------------------------------------------------------------------- */
+
+/* The arena's CUDA IPC handle (64 bytes into `handle`), for the other
+ * GPUs' processes to map it with b200shm_peer_open.  Every engine of a
+ * spanning job is initialised with the same npes and heap size (the
+ * symmetric heap's own rule), and not in managed memory.  The reference
+ * reaches other PEs' heaps through UCX rkeys (src/shmemc/ucx/comms.c:58-112);
+ * here another GPU's arena is one mapped address range. */
+int b200shm_ipc_handle(void *handle);
+/* Map another engine's arena from its IPC handle; *peer_base receives the
+ * device address of its slice 0. */
+int b200shm_peer_open(const void *handle, void **peer_base);
+int b200shm_peer_close(void *peer_base);
+
+/* The cross-GPU half of a reduction over a team of G x pe_count members
+ * (pe_count on each of G GPUs, G a power of two up to 16), fused with its
+ * write-back: element by element, the G ranks' partial vectors -- each the
+ * reduction over one GPU's members, at the device addresses partials[g]
+ * (this rank's own, the others' through b200shm_peer_open) -- combined as
+ * rank `rank` combines them in the butterfly (round j pairs rank r with
+ * r ^ 2^j, keeping op(own, partner): src/shcoll/src/reduce.c:250-272), the
+ * result written to this GPU's members pe_start + i*pe_stride at dest_off.
+ * Plain loads of the peers' memory.  The caller separates the phases with a
+ * barrier across the processes: all partials written before any rank
+ * combines, all combines done before any partial is overwritten.  Every
+ * dtype but long double; complex for SUM and PROD only. */
+int b200shm_span_combine(int op, int dtype, int G, int rank, const uint64_t *partials,
+                         int pe_start, int pe_stride, int pe_count, uint64_t dest_off,
+                         uint64_t nelems, void *stream);
+/* fcollect over the same team: member m = g*pe_count + k (on GPU g) sends
+ * nbytes from src_off; every local member's dest holds the G*pe_count
+ * blocks in member order.  bases[g] = GPU g's arena base (this rank's own
+ * b200shm_heap_base, the others' mapped).  Replaces fcollect_helper_*
+ * (src/shcoll/src/fcollect.c:32-484) for a team across GPUs. */
+int b200shm_span_fcollect(int G, int rank, const uint64_t *bases, int pe_start, int pe_stride,
+                          int pe_count, uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
+                          void *stream);
+/* alltoall over the same team: local member j's dest block m = member m's
+ * source block rank*pe_count + j, wherever member m lives.  Replaces
+ * alltoall_helper_* (src/shcoll/src/alltoall.c:75-201) across GPUs. */
+int b200shm_span_alltoall(int G, int rank, const uint64_t *bases, int pe_start, int pe_stride,
+                          int pe_count, uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
+                          void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* batched reductions                                                      */
 /* ---------------------------------------------------------------------- */
 

@@ -91,6 +91,12 @@ def _load():
         "b200shm_serve_replay": (ci, [vp, vp, u64, vp, vp, vp]),
         "b200shm_serve_replay_ordered": (ci, [vp, u64, vp, ctypes.POINTER(ctypes.c_double), vp]),
         "b200shm_amo": (ci, [ci, ci, ci, u64, vp, vp, vp]),
+        "b200shm_ipc_handle": (ci, [vp]),
+        "b200shm_peer_open": (ci, [vp, ctypes.POINTER(vp)]),
+        "b200shm_peer_close": (ci, [vp]),
+        "b200shm_span_combine": (ci, [ci, ci, ci, ci, vp, ci, ci, ci, u64, u64, vp]),
+        "b200shm_span_fcollect": (ci, [ci, ci, vp, ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_span_alltoall": (ci, [ci, ci, vp, ci, ci, ci, u64, u64, u64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -233,6 +239,61 @@ def alltoalls(dest, src, dst, sst, nelems, elem_size, team=None, stream=None):
     start, stride, size = _team(team)
     return _check(lib.b200shm_alltoalls(start, stride, size, dest, src, dst, sst, nelems,
                                         elem_size, stream))
+
+
+def heap_slice():
+    return lib.b200shm_heap_slice()
+
+
+def heap_base():
+    """Device address of slice 0 of this process's arena."""
+    return lib.b200shm_heap_base() or 0
+
+
+def ipc_handle():
+    """The arena's CUDA IPC handle (64 bytes) for another process to map."""
+    h = ctypes.create_string_buffer(64)
+    _check(lib.b200shm_ipc_handle(h))
+    return h.raw
+
+
+def peer_open(handle):
+    """Map another process's arena; returns the device address of its slice 0."""
+    base = ctypes.c_void_p()
+    _check(lib.b200shm_peer_open(bytes(handle), ctypes.byref(base)))
+    return base.value
+
+
+def peer_close(base):
+    return _check(lib.b200shm_peer_close(base))
+
+
+def _addrs(addrs):
+    a = np.ascontiguousarray(addrs, dtype=np.uint64)
+    return a, a.ctypes.data
+
+
+def span_combine(op, dtype, G, rank, partials, dest, nelems, team=None, stream=None):
+    """The cross-GPU butterfly levels over G partial vectors at the device
+    addresses `partials`, written to this GPU's team members at `dest`."""
+    start, stride, size = _team(team)
+    a, ap = _addrs(partials)
+    return _check(lib.b200shm_span_combine(OPS.index(op), DTYPES.index(dtype), G, rank, ap, start,
+                                           stride, size, dest, nelems, stream))
+
+
+def span_fcollect(G, rank, bases, dest, src, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    a, ap = _addrs(bases)
+    return _check(lib.b200shm_span_fcollect(G, rank, ap, start, stride, size, dest, src, nbytes,
+                                            stream))
+
+
+def span_alltoall(G, rank, bases, dest, src, nbytes, team=None, stream=None):
+    start, stride, size = _team(team)
+    a, ap = _addrs(bases)
+    return _check(lib.b200shm_span_alltoall(G, rank, ap, start, stride, size, dest, src, nbytes,
+                                            stream))
 
 
 def broadcast(root, dest, src, nbytes, team=None, stream=None):

@@ -37,10 +37,16 @@ the rank that owns their target member and run there as one batch, their
 old values returned in the caller's order.  All three are byte-exact for
 any team.
 
-Step 2 moves N elements per round over NCCL (point-to-point over NVLink);
-no TMA multicast is used anywhere on this path.  Nothing here has run on
-more than one GPU: this pool gives one GPU per job, so the cross-rank
-steps are exercised with gloo ranks on the CPU (tests/test_spanning_team.py).
+SpanningTeam's step 2 moves N elements per round through torch.distributed
+(NCCL point-to-point over NVLink on GPUs).  PeerTeam does the cross-GPU
+steps in the engine instead: the ranks map each other's arenas through CUDA
+IPC, and one kernel per rank reads the other ranks' partials (or blocks)
+with plain loads and writes its own members -- the butterfly's cross-GPU
+levels fused with the write-back.  No TMA multicast is used anywhere on
+this path.  The cross-rank logic runs on gloo ranks on the CPU
+(tests/test_spanning_team.py, tests/test_peer_team_cpu.py); PeerTeam's
+kernels run as 2 and 4 processes sharing one GPU, which is sound because no
+kernel waits on another rank's (tests/test_peer_team_gpu.py).
 """
 import torch
 import torch.distributed as dist
@@ -287,6 +293,111 @@ class SpanningTeam:
         out = torch.empty(len(pe), dtype=torch.int64)
         out[order] = back.cpu()
         return out
+
+
+class PeerTeam(SpanningTeam):
+    """The spanning team with its cross-GPU steps as kernels of the engine
+    that read the other ranks' arenas directly, through CUDA IPC mappings
+    (b200shm_ipc_handle / b200shm_peer_open): plain loads over NVLink, no
+    multicast, and no copy through a collective library.
+
+    Every rank's engine has the same npes and heap size and is not in
+    managed memory; G = the group's size is a power of two up to 16.  The
+    host keeps the phases apart with a barrier across the ranks (the
+    device synchronised, then the group's barrier), so no kernel waits on
+    another GPU's kernel:
+
+      reduce    the local members' reduction into a scratch object
+                (step 1), barrier, then b200shm_span_combine on every rank:
+                the butterfly's cross-GPU levels over the G partials, read
+                from the G arenas, fused with the write of the result to the
+                local members' dest (steps 2 and 3 in one kernel), barrier
+                (before the scratch is written again).  Long vectors go in
+                chunks of the scratch's size.
+      fcollect  barrier (every rank's source written), one kernel per rank
+                reading every member's block from the GPU that holds it and
+                writing the local members' dest, barrier (before any source
+                is overwritten).
+      alltoall  the same, each local member's dest blocks read from the
+                members that hold them.
+
+    Results are those of SpanningTeam: the same combine order, so the same
+    bits (`exact`); byte-exact data movement.  Atomics keep the routed
+    form of SpanningTeam.
+    """
+
+    def __init__(self, engine, members_per_rank, group=None, local_start=0, local_stride=1,
+                 scratch_bytes=1 << 22):
+        super().__init__(engine, members_per_rank, group, local_start, local_stride)
+        G = self.world
+        if not _pow2(G) or G > 16:
+            raise ValueError("PeerTeam: %d ranks (a power of two up to 16)" % G)
+        self.scratch_bytes = scratch_bytes
+        self.scratch = engine.malloc(scratch_bytes)
+        mine = (engine.ipc_handle(), engine.heap_slice(), engine.n_pes(), self.local,
+                self.scratch)
+        infos = [None] * G
+        dist.all_gather_object(infos, mine, group=group)
+        # every rank sees the same table, so every rank refuses together
+        if len({(i[1], i[2], i[3]) for i in infos}) != 1:
+            engine.free(self.scratch)
+            raise ValueError("PeerTeam: every rank needs the same npes, heap size and local team")
+        self.slice = mine[1]
+        self.bases = [engine.heap_base() if r == self.rank else engine.peer_open(info[0])
+                      for r, info in enumerate(infos)]
+        self.scratch_of = [info[4] for info in infos]
+
+    def barrier(self):
+        self.sync_device()
+        dist.barrier(group=self.group)
+
+    def close(self):
+        """Unmap the peers' arenas and free the scratch (all ranks together)."""
+        self.barrier()
+        for r, b in enumerate(self.bases):
+            if r != self.rank:
+                self.B.peer_close(b)
+        self.B.free(self.scratch)
+        self.bases = []
+        dist.barrier(group=self.group)
+
+    def reduce(self, op, dtype, algo, dest, src, nelems):
+        """All-reduce over the spanning team; returns True when the result is
+        bit-identical to the reference's (see `exact`)."""
+        start, stride, L = self.local
+        es = torch.empty((), dtype=_TORCH[dtype]).element_size() if dtype in _TORCH else \
+            {"complex64": 8, "complex128": 16}[dtype]
+        chunk = self.scratch_bytes // es
+        partials = [self.bases[g] + start * self.slice + self.scratch_of[g]
+                    for g in range(self.world)]
+        e0 = 0
+        while e0 < nelems:
+            n = min(chunk, nelems - e0)
+            self.B.reduce(op, dtype, algo, self.scratch, src + e0 * es, n, team=self.local)
+            self.barrier()
+            self.B.span_combine(op, dtype, self.world, self.rank, partials, dest + e0 * es, n,
+                                team=self.local)
+            self.barrier()
+            e0 += n
+        return self.exact(op, dtype, algo)
+
+    def fcollect(self, dest, src, nbytes):
+        """Every member's dest holds the P members' blocks in member order
+        (fcollect_helper_*, src/shcoll/src/fcollect.c:32-484), each block
+        read once from the GPU that holds it."""
+        self.barrier()
+        self.B.span_fcollect(self.world, self.rank, self.bases, dest, src, nbytes,
+                             team=self.local)
+        self.barrier()
+
+    def alltoall(self, dest, src, nbytes):
+        """Member j's dest block k = member k's source block j
+        (alltoall_helper_*, src/shcoll/src/alltoall.c:75-201), read from
+        whichever GPU holds member k."""
+        self.barrier()
+        self.B.span_alltoall(self.world, self.rank, self.bases, dest, src, nbytes,
+                             team=self.local)
+        self.barrier()
 
 
 _TORCH = {"int8": torch.int8, "int16": torch.int16, "int32": torch.int32, "int64": torch.int64,

@@ -1,0 +1,176 @@
+"""A team spanning GPUs through peer memory (spanning.PeerTeam): its ranks
+are processes that map each other's arenas with CUDA IPC, and its
+cross-rank steps are the engine's span kernels (b200shm_span_combine,
+b200shm_span_fcollect, b200shm_span_alltoall) reading the other ranks'
+arenas with plain loads.
+
+The ranks run here as 2 and 4 processes on one GPU.  That is sound for
+these kernels: none of them waits on another rank's kernel (host barriers
+over a gloo group separate every phase), so they need not run at the same
+time.  Each rank holds `L` members of a team of world x L; the results on
+every rank's members are compared with the oracle over the whole team: bit
+for bit where the team's `exact` says so (and it must say so for every
+integer case and the butterfly float cases here), else within
+P * eps * sum|x|."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.abspath(__file__)) + "/.."
+
+# (op, dtype, algo, nelems); the scratch object is 64 KiB, so the longer
+# vectors go through the combine in several chunks
+CASES = [("sum", "float32", "rec_dbl", 40000), ("sum", "float64", "rabenseifner", 3001),
+         ("prod", "float64", "rec_dbl", 777), ("xor", "int64", "linear", 5000),
+         ("min", "int32", "rec_dbl", 4097), ("max", "float32", "binomial", 1000),
+         ("sum", "uint64", "rabenseifner2", 2500), ("sum", "int8", "rec_dbl", 20003),
+         ("and", "uint16", "linear", 999), ("sum", "complex64", "rec_dbl", 1000),
+         ("prod", "complex128", "rec_dbl", 300), ("sum", "float32", "linear", 3000),
+         ("max", "uint8", "binomial", 17)]
+L = 4                       # members per rank: PEs 1, 3, 5, 7 of each engine
+LOCAL = (1, 2, L)
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def inputs(op, dtype, P, n, seed):
+    import gen
+    dt = np.dtype(dtype)
+    if dt.kind in "iu":
+        lo, hi = (-3, 3) if op == "prod" else (None, None)
+        return gen.uniform_int(dt, P, n, seed, lo, hi)
+    if dt.kind == "c":
+        if op == "prod":
+            re = gen.uniform(np.float64, P, n, seed, 0.99, 1.01)
+            im = gen.uniform(np.float64, P, n, seed + 1, -0.01, 0.01)
+        else:
+            re, im = gen.normal(np.float64, P, n, seed), gen.normal(np.float64, P, n, seed + 1)
+        return (re + 1j * im).astype(dt)
+    if op == "prod":
+        return gen.uniform(dt, P, n, seed, 0.99, 1.01)
+    return gen.normal(dt, P, n, seed)
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    for p in (os.path.join(ROOT, "osss-ucx_b200"), os.path.join(ROOT, "oracle"),
+              os.path.join(ROOT, "tests")):
+        sys.path.insert(0, p)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    res = []
+    try:
+        import b200shm as B
+        import oracle
+        import spanning
+        torch.cuda.set_device(0)
+        B.init(8, 8 << 20)
+        rs = oracle.Restatement()
+        P = world * L
+        mine = slice(rank * L, (rank + 1) * L)
+
+        # an engine that disagrees about the local team: every rank refuses
+        try:
+            spanning.PeerTeam(B, L, local_start=1, local_stride=1 + (rank == world - 1))
+            res.append(("mismatch", -1, False, "not refused"))
+        except ValueError:
+            res.append(("mismatch", -1, True, ""))
+
+        t = spanning.PeerTeam(B, L, local_start=LOCAL[0], local_stride=LOCAL[1],
+                              scratch_bytes=1 << 16)
+        for k, (op, dtype, algo, n) in enumerate(CASES):
+            x = inputs(op, dtype, P, n, 1000 * world + k)
+            nb = x[0].nbytes
+            src, dst = B.malloc(nb), B.malloc(nb)
+            B.put_rows(src, x[mine], team=LOCAL)
+            B.memset(dst, 0x5A, nb, team=LOCAL)
+            before = B.launch_count()
+            exact = t.reduce(op, dtype, algo, dst, src, n)
+            launched = B.launch_count() - before
+            got = B.get_rows(dst, nb, x.dtype, team=LOCAL)
+            want = rs.reduce(algo, op, x)[mine]
+            if exact:
+                ok = got.tobytes() == want.tobytes()
+            else:
+                w = x.astype(np.complex128 if x.dtype.kind == "c" else np.float64)
+                ref = w.sum(0) if op == "sum" else w.prod(0)
+                eps = np.finfo(x.real.dtype).eps
+                bound = P * eps * np.abs(w).sum(0)
+                ok = bool((np.abs(got.astype(w.dtype) - ref) <= bound).all())
+            res.append(("reduce", k, bool(ok) and launched >= 2, (bool(exact), launched)))
+            B.free(src)
+            B.free(dst)
+
+        rng = np.random.default_rng(7 + world)
+        for nb in (48, 4096, 3):
+            x = rng.integers(0, 256, (P, P * nb), dtype=np.uint8)
+            src, dst = B.malloc(P * nb), B.malloc(P * nb)
+            B.put_rows(src, x[mine], team=LOCAL)
+            B.memset(dst, 0xA5, P * nb, team=LOCAL)
+            t.fcollect(dst, src, nb)
+            want = rs.fcollect(np.ascontiguousarray(x[:, :nb]))[mine]
+            got = B.get_rows(dst, P * nb, np.uint8, team=LOCAL)
+            res.append(("fcollect", nb, got.tobytes() == want.tobytes(), ""))
+            B.memset(dst, 0xA5, P * nb, team=LOCAL)
+            t.alltoall(dst, src, nb)
+            want = rs.alltoall(x)[mine]
+            got = B.get_rows(dst, P * nb, np.uint8, team=LOCAL)
+            res.append(("alltoall", nb, got.tobytes() == want.tobytes(), ""))
+            B.free(src)
+            B.free(dst)
+        t.close()
+    except Exception as e:  # reported, then the group is left in order
+        res.append(("error", -1, False, repr(e)))
+    try:
+        dist.barrier()
+        dist.destroy_process_group()
+    finally:
+        q.put((rank, res))
+
+
+def run_world(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    ps = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    out = dict(q.get(timeout=600) for _ in ps)
+    for p in ps:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 4])
+def test_peer_team_matches_oracle(world):
+    """reduce (every dtype class, butterfly and other orders, several
+    chunks), fcollect and alltoall (16-byte and byte paths) over world x 4
+    members, each rank's members checked against the oracle."""
+    out = run_world(world)
+    assert sorted(out) == list(range(world))
+    for rank, res in out.items():
+        assert res and res[-1][0] != "error", (world, rank, res[-1])
+        for kind, k, ok, detail in res:
+            assert ok, (world, rank, kind, k, detail,
+                        CASES[k] if kind == "reduce" else None)
+        n_red = sum(1 for r in res if r[0] == "reduce")
+        assert n_red == len(CASES)
+        for kind, k, ok, (exact, _) in (r for r in res if r[0] == "reduce"):
+            op, dtype, algo, _n = CASES[k]
+            want_exact = (not (dtype.startswith("float") or dtype.startswith("complex"))
+                          or op in ("min", "max")
+                          or algo in ("rec_dbl", "rabenseifner", "rabenseifner2"))
+            assert exact == want_exact, (world, CASES[k])
