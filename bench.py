@@ -226,10 +226,11 @@ def main():
     ap.add_argument("--heap-mb", type=int, default=HEAP >> 20, help="heap slice per PE (MiB)")
     ap.add_argument("--nelems", type=int, default=N, help="elements per PE")
     ap.add_argument("--workload", default="reduce",
-                    choices=["reduce", "movement", "batch", "serve"],
+                    choices=["reduce", "movement", "batch", "serve", "span"],
                     help="reduce (headline), movement (alltoall/alltoalls/fcollect/AMO), "
-                         "batch (4096 reductions over 512 teams of 2048 PEs) or serve "
-                         "(open-loop request stream over 256 PEs)")
+                         "batch (4096 reductions over 512 teams of 2048 PEs), serve "
+                         "(open-loop request stream over 256 PEs) or span (the kernels of a "
+                         "team spanning 8 GPUs, the 8 arenas emulated on one GPU)")
     ap.add_argument("--serve-requests", type=int, default=100000)
     ap.add_argument("--serve-rate", type=float, default=200000.0, help="arrivals per second")
     ap.add_argument("--serve-percall", type=int, default=20000,
@@ -243,7 +244,7 @@ def main():
                     help="movement workload: PEs (128 is the configuration; 64 keeps profiling "
                          "captures to a few GB)")
     ap.add_argument("--headline-only", action="store_true",
-                    help="skip the config1/movement/batch/serve sub-objects of the default line")
+                    help="skip the config1/movement/batch/serve/span sub-objects of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -258,7 +259,8 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.workload != "reduce":
-        fn = {"movement": run_movement, "batch": run_batch, "serve": run_serve}[args.workload]
+        fn = {"movement": run_movement, "batch": run_batch, "serve": run_serve,
+              "span": run_span}[args.workload]
         line = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
@@ -400,7 +402,7 @@ def main():
         # the other configurations, each in its own arena, after the headline
         B.finalize()
         for name, fn in (("config1", run_config1), ("movement", run_movement),
-                         ("batch", run_batch), ("serve", run_serve)):
+                         ("batch", run_batch), ("serve", run_serve), ("span", run_span)):
             t0 = time.perf_counter()
             try:
                 extras[name] = fn(args, world, rank, local)
@@ -675,6 +677,103 @@ def run_movement(args, world, rank, local):
                        "fcollect64_nelems": NF, "amo": "2^20 fetch_add int64 on 2^20 counters/PE",
                        "l2": "every copy moves >= 512 MiB (> L2); the AMO counters span 1 GiB"},
             "results": res, "gpu_launches": launches, "cpu_baseline": cpu}
+
+
+# ---------------------------------------------------------------------------
+# the span kernels: a team of 64 members over 8 GPUs (8 per GPU)
+# ---------------------------------------------------------------------------
+def run_span(args, world, rank, local, G=8, L=8, NC=1 << 23, FB=256 << 10, AB=256 << 10):
+    """The cross-GPU kernels of a team spanning G=8 GPUs with L=8 members on
+    each, as rank 0 runs them -- b200shm_span_combine (the butterfly's
+    cross-GPU levels over 8 partial vectors of 2^23 float32, SUM, written to
+    the 8 local members), b200shm_span_fcollect (64 blocks of 256 KiB) and
+    b200shm_span_alltoall (64 x 8 blocks of 256 KiB) -- with the 8 ranks'
+    arenas emulated as disjoint slice ranges of one 64-PE arena (rank g's
+    members are PEs 8g..8g+7), so every load is a local HBM load.  Across
+    GPUs 7/8 of the loads cross NVLink instead.  Timed with CUDA events,
+    checked against the oracle (the combine is rank 0's rec_dbl result over
+    the 8 partials)."""
+    import torch
+    import __graft_entry__
+    __graft_entry__.build_library()
+    import b200shm as B
+    import gen
+    import oracle
+    rs = oracle.Restatement()
+    P = G * L
+    B.init(P, 128 << 20)  # 8 GiB: 113 MiB of objects per PE
+    try:
+        slice_ = B.heap_slice()
+        base = B.heap_base()
+        bases = [base + g * L * slice_ for g in range(G)]
+        local_team = (0, 1, L)
+        s_ptr = B.stream()
+        st = torch.cuda.ExternalStream(s_ptr)
+        part, dst = B.malloc(NC * 4), B.malloc(NC * 4)
+        xs = gen.normal(np.float32, G, NC, 41)
+        for g in range(G):  # rank g's partial in its member 0 (PE 8g)
+            B.put_rows(part, xs[g:g + 1], team=(g * L, 1, 1))
+        partials = [B.ptr(g * L, part) for g in range(G)]
+        fsrc, fdst = B.malloc(FB), B.malloc(P * FB)
+        asrc, adst = B.malloc(P * AB), B.malloc(P * AB)
+        fx = gen.uniform_int(np.uint8, P, FB, 42)
+        ax = gen.uniform_int(np.uint8, P, P * AB, 43)
+        B.put_rows(fsrc, fx, team=(0, 1, P))
+        B.put_rows(asrc, ax, team=(0, 1, P))
+        peak, peak_kind = peaks()
+        ops = {
+            "combine_f32_sum": (lambda: B.span_combine("sum", "float32", G, 0, partials, dst, NC,
+                                                       team=local_team, stream=s_ptr),
+                                (G + L) * NC * 4, "k_span_combine"),
+            "fcollect": (lambda: B.span_fcollect(G, 0, bases, fdst, fsrc, FB, team=local_team,
+                                                 stream=s_ptr),
+                         P * FB + L * P * FB, "k_span_fcollect"),
+            "alltoall": (lambda: B.span_alltoall(G, 0, bases, adst, asrc, AB, team=local_team,
+                                                 stream=s_ptr),
+                         2 * L * P * AB, "k_span_alltoall"),
+        }
+        traffic = {}
+        tpath = os.path.join(ROOT, "profiles", "span_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f)
+        res = {}
+        launches0 = B.launch_count()
+        for name, (fn, nbytes, kern) in ops.items():
+            for _ in range(args.warmup):
+                fn()
+            B.quiet()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                fn()
+            e1.record(st)
+            B.quiet()
+            ms = e0.elapsed_time(e1) / args.steps
+            gbs = nbytes / (ms / 1e3) / 1e9
+            res[name] = {"kernel": kern, "ms": round(ms, 4), "bytes_per_launch": nbytes,
+                         "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak,
+                                      "unit": "GB/s", "frac": round(gbs / peak, 4),
+                                      "traffic": traffic.get(name)}}
+        launches = B.launch_count() - launches0
+        want = rs.reduce("rec_dbl", "sum", xs)[0]
+        got = B.get_rows(dst, NC * 4, np.float32, team=local_team)
+        res["combine_f32_sum"]["bit_exact"] = all(r.tobytes() == want.tobytes() for r in got)
+        del got
+        want = rs.fcollect(fx)[:L]
+        got = B.get_rows(fdst, P * FB, np.uint8, team=local_team)
+        res["fcollect"]["bit_exact"] = got.tobytes() == want.tobytes()
+        want = rs.alltoall(ax)[:L]
+        got = B.get_rows(adst, P * AB, np.uint8, team=local_team)
+        res["alltoall"]["bit_exact"] = got.tobytes() == want.tobytes()
+    finally:
+        B.finalize()
+    return {"workload": "span", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "config": {"ranks": G, "members_per_rank": L, "combine": "2^23 float32 SUM",
+                       "fcollect_block": FB, "alltoall_block": AB,
+                       "arenas": "8 ranks emulated as slice ranges of one arena (local loads)",
+                       "l2": "each launch moves >= 144 MiB (> L2)"},
+            "peak_gbs": peak, "peak_kind": peak_kind, "results": res, "gpu_launches": launches}
 
 
 # ---------------------------------------------------------------------------
