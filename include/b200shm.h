@@ -280,6 +280,20 @@ int b200shm_span_alltoall(int G, int rank, const uint64_t *bases, int pe_start, 
                           int pe_count, uint64_t dest_off, uint64_t src_off, uint64_t nbytes,
                           void *stream);
 
+/* One-sided atomics over the same team: op k on member member[k] (on GPU
+ * member[k] / pe_count) at byte offset off[k], run by this GPU as a
+ * system-scope atomic on the owner's arena -- the other GPUs' through
+ * b200shm_peer_open, over NVLink -- with no other rank taking part; the
+ * old values land in fetched[k] (device arrays, as b200shm_amo_batch).
+ * Ops of different GPUs on one word are applied atomically in an
+ * unspecified order, as concurrent AMOs of different PEs are in OpenSHMEM
+ * (src/shmemc/ucx/comms.c:409-671).  A target outside the team or the
+ * slice fails the call with B200SHM_ERR_ARG after the others ran. */
+int b200shm_span_amo(int amo, int dtype, int G, const uint64_t *bases, int pe_start,
+                     int pe_stride, int pe_count, uint64_t nops, const int32_t *member,
+                     const uint64_t *off, const void *value, const void *cond, void *fetched,
+                     void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* batched reductions                                                      */
 /* ---------------------------------------------------------------------- */

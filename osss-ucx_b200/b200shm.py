@@ -97,6 +97,7 @@ def _load():
         "b200shm_span_combine": (ci, [ci, ci, ci, ci, vp, ci, ci, ci, u64, u64, vp]),
         "b200shm_span_fcollect": (ci, [ci, ci, vp, ci, ci, ci, u64, u64, u64, vp]),
         "b200shm_span_alltoall": (ci, [ci, ci, vp, ci, ci, ci, u64, u64, u64, vp]),
+        "b200shm_span_amo": (ci, [ci, ci, ci, vp, ci, ci, ci, u64, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -294,6 +295,17 @@ def span_alltoall(G, rank, bases, dest, src, nbytes, team=None, stream=None):
     a, ap = _addrs(bases)
     return _check(lib.b200shm_span_alltoall(G, rank, ap, start, stride, size, dest, src, nbytes,
                                             stream))
+
+
+def span_amo(amo, dtype, G, bases, nops, member_dev, off_dev, value_dev=None, cond_dev=None,
+             fetched_dev=None, team=None, stream=None):
+    """One-sided atomics on any member of a spanning team (device arrays:
+    int32 members, uint64 byte offsets, 4- or 8-byte operands)."""
+    start, stride, size = _team(team)
+    a, ap = _addrs(bases)
+    return _check(lib.b200shm_span_amo(AMOS.index(amo), DTYPES.index(dtype), G, ap, start, stride,
+                                       size, nops, member_dev, off_dev, value_dev, cond_dev,
+                                       fetched_dev, stream))
 
 
 def broadcast(root, dest, src, nbytes, team=None, stream=None):

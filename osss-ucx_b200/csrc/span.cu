@@ -23,7 +23,11 @@
  *    (src/shcoll/src/fcollect.c:32-484);
  *  - b200shm_span_alltoall: each local member's dest blocks, read from the
  *    members that hold them on whichever GPU (src/shcoll/src/alltoall.c:
- *    75-201).
+ *    75-201);
+ *  - b200shm_span_amo: one-sided atomics on any member's words, run by the
+ *    calling GPU as system-scope atomics on the owner's arena (the
+ *    reference's shmemc_ctx_{fadd,...} over UCX, src/shmemc/ucx/comms.c:
+ *    409-671): no other rank takes part.
  */
 #include <stdint.h>
 #include <string.h>
@@ -173,6 +177,51 @@ __global__ void __launch_bounds__(256) k_span_alltoall(const __grid_constant__ S
       if constexpr (VEC) st16(dst + v * 16, ld16(src + v * 16));
       else dst[v] = src[v];
     }
+  }
+}
+
+/* one AMO as a system-scope atomic: the word may be updated at the same
+ * time by kernels of other GPUs through their mappings of this arena, and
+ * only system scope makes those updates atomic with each other */
+template <class W>
+__device__ __forceinline__ W amo_sys(int amo, W *p, W v, W c) {
+  switch (amo) {
+  case B200SHM_AMO_FETCH_ADD:
+  case B200SHM_AMO_ADD: return atomicAdd_system(p, v);
+  case B200SHM_AMO_FETCH_INC:
+  case B200SHM_AMO_INC: return atomicAdd_system(p, (W)1);
+  case B200SHM_AMO_SWAP:
+  case B200SHM_AMO_SET: return atomicExch_system(p, v);
+  case B200SHM_AMO_CSWAP: return atomicCAS_system(p, c, v);
+  case B200SHM_AMO_FETCH: return atomicAdd_system(p, (W)0);
+  case B200SHM_AMO_FETCH_AND:
+  case B200SHM_AMO_AND: return atomicAnd_system(p, v);
+  case B200SHM_AMO_FETCH_OR:
+  case B200SHM_AMO_OR: return atomicOr_system(p, v);
+  default: return atomicXor_system(p, v);
+  }
+}
+
+/* atomics on (member, offset) targets of a spanning team: member m = q*L +
+ * k is PE first/slice + k*step/slice of GPU q's arena */
+template <class W>
+__global__ void __launch_bounds__(256) k_span_amo(const __grid_constant__ SpanPtrs base, int M,
+                                                  int L, uint64_t first, uint64_t step,
+                                                  uint64_t slice, int amo, uint64_t nops,
+                                                  const int32_t *member, const uint64_t *off,
+                                                  const W *value, const W *cond, W *fetched,
+                                                  int *status) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nops;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const int m = member[k];
+    const uint64_t o = off[k];
+    if (m < 0 || m >= M || o > slice - sizeof(W) || (o % sizeof(W)) != 0) {
+      atomicOr(status, (int)B200SHM_STATUS_BADREQ);
+      continue;
+    }
+    W *t = (W *)(base.p[m / L] + first + (uint64_t)(m % L) * step + o);
+    const W old = amo_sys<W>(amo, t, value ? value[k] : (W)0, cond ? cond[k] : (W)0);
+    if (fetched) fetched[k] = old;
   }
 }
 
@@ -360,6 +409,45 @@ int b200shm_span_alltoall(int G, int rank, const uint64_t *bases, int pe_start, 
                                                 dest_off, src_off, nbytes);
   count_launch();
   return finish(stream, "b200shm_span_alltoall");
+}
+
+int b200shm_span_amo(int amo, int dtype, int G, const uint64_t *bases, int pe_start,
+                     int pe_stride, int pe_count, uint64_t nops, const int32_t *member,
+                     const uint64_t *off, const void *value, const void *cond, void *fetched,
+                     void *stream) {
+  int rc = span_check(G, 0, bases, pe_start, pe_stride, pe_count);
+  if (rc) return rc;
+  if (amo < 0 || amo >= B200SHM_AMO_NOP) return fail(B200SHM_ERR_ARG, "span_amo: unknown op %d", amo);
+  const bool w4 = dtype == B200SHM_I32 || dtype == B200SHM_U32 || dtype == B200SHM_F32;
+  const bool w8 = dtype == B200SHM_I64 || dtype == B200SHM_U64 || dtype == B200SHM_F64;
+  if (!w4 && !w8) return fail(B200SHM_ERR_UNSUPPORTED, "span_amo: dtype %d is not 4 or 8 bytes", dtype);
+  const bool is_float = dtype == B200SHM_F32 || dtype == B200SHM_F64;
+  if (is_float && amo != B200SHM_AMO_SWAP && amo != B200SHM_AMO_SET && amo != B200SHM_AMO_FETCH)
+    return fail(B200SHM_ERR_UNSUPPORTED, "span_amo: floating types support only swap/set/fetch");
+  const bool needs_value = !(amo == B200SHM_AMO_FETCH || amo == B200SHM_AMO_INC ||
+                             amo == B200SHM_AMO_FETCH_INC);
+  if (nops == 0) return B200SHM_OK;
+  if (!member || !off || (needs_value && !value) || (amo == B200SHM_AMO_CSWAP && !cond))
+    return fail(B200SHM_ERR_ARG, "span_amo: missing operand array");
+  SpanPtrs p{};
+  for (int g = 0; g < G; g++) p.p[g] = (const char *)(uintptr_t)bases[g];
+  const uint64_t first = (uint64_t)pe_start * st().slice;
+  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
+  const int M = G * pe_count;
+  const unsigned grid = grid_for(nops, 256, 8);
+  cudaStream_t s = pick_stream(stream);
+  if (w8)
+    k_span_amo<unsigned long long><<<grid, 256, 0, s>>>(
+        p, M, pe_count, first, step, st().slice, amo, nops, member, off,
+        (const unsigned long long *)value, (const unsigned long long *)cond,
+        (unsigned long long *)fetched, st().d_status);
+  else
+    k_span_amo<unsigned int><<<grid, 256, 0, s>>>(
+        p, M, pe_count, first, step, st().slice, amo, nops, member, off,
+        (const unsigned int *)value, (const unsigned int *)cond, (unsigned int *)fetched,
+        st().d_status);
+  count_launch();
+  return finish(stream, "b200shm_span_amo");
 }
 
 }  // extern "C"

@@ -249,7 +249,8 @@ class SpanningTeam:
         pe = (start + pe_local.to(torch.int64) * stride).to(torch.int32).cuda()
         o = off.to(torch.int64).cuda()  # byte offsets, read by the engine as uint64
         v = value.to(torch.int64).cuda()
-        f = torch.zeros(n, dtype=torch.int64, device="cuda")
+        # written whole by the engine's stream: no fill kernel on torch's
+        f = torch.empty(n, dtype=torch.int64, device="cuda")
         self.B.amo_batch(amo, dtype, n, pe.data_ptr(), o.data_ptr(), v.data_ptr(), None,
                          f.data_ptr())
         return f.cpu()
@@ -320,10 +321,11 @@ class PeerTeam(SpanningTeam):
                 is overwritten).
       alltoall  the same, each local member's dest blocks read from the
                 members that hold them.
+      amo       one-sided: system-scope atomics on the owner's arena, run
+                by the calling GPU alone (no barrier, no exchange).
 
     Results are those of SpanningTeam: the same combine order, so the same
-    bits (`exact`); byte-exact data movement.  Atomics keep the routed
-    form of SpanningTeam.
+    bits (`exact`); byte-exact data movement; atomics exact.
     """
 
     def __init__(self, engine, members_per_rank, group=None, local_start=0, local_stride=1,
@@ -380,6 +382,29 @@ class PeerTeam(SpanningTeam):
             self.barrier()
             e0 += n
         return self.exact(op, dtype, algo)
+
+    def amo(self, amo, dtype, pe, off, value, cond=None):
+        """One-sided atomics on (member, offset) targets anywhere in the
+        team: this GPU runs every op as a system-scope atomic on the owner's
+        arena (peer memory for members on other GPUs), with no exchange and
+        no other rank taking part; returns the old values (int64, on the CPU,
+        in the caller's order).  Ops of different ranks on one word are
+        applied atomically in an unspecified order (src/shmemc/ucx/comms.c:
+        409-671).  dtype: 4- or 8-byte."""
+        wide = dtype in ("int64", "uint64", "float64")
+        tdt = torch.int64 if wide else torch.int32
+        n = len(pe)
+        if n == 0:
+            return torch.zeros(0, dtype=torch.int64)
+        member = torch.as_tensor(pe, dtype=torch.int64).to(torch.int32).cuda()
+        o = torch.as_tensor(off, dtype=torch.int64).cuda()
+        v = torch.as_tensor(value, dtype=torch.int64).to(tdt).cuda()
+        c = None if cond is None else torch.as_tensor(cond, dtype=torch.int64).to(tdt).cuda()
+        f = torch.empty(n, dtype=tdt, device="cuda")  # written whole by the engine
+        self.B.span_amo(amo, dtype, self.world, self.bases, n, member.data_ptr(), o.data_ptr(),
+                        v.data_ptr(), None if c is None else c.data_ptr(), f.data_ptr(),
+                        team=self.local)
+        return f.cpu().to(torch.int64)
 
     def fcollect(self, dest, src, nbytes):
         """Every member's dest holds the P members' blocks in member order

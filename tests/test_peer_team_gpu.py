@@ -2,7 +2,8 @@
 are processes that map each other's arenas with CUDA IPC, and its
 cross-rank steps are the engine's span kernels (b200shm_span_combine,
 b200shm_span_fcollect, b200shm_span_alltoall) reading the other ranks'
-arenas with plain loads.
+arenas with plain loads, and its atomics one-sided system-scope atomics on
+the owner's arena (b200shm_span_amo).
 
 The ranks run here as 2 and 4 processes on one GPU.  That is sound for
 these kernels: none of them waits on another rank's kernel (host barriers
@@ -128,6 +129,38 @@ def _rank_main(rank, world, port, q):
             res.append(("alltoall", nb, got.tobytes() == want.tobytes(), ""))
             B.free(src)
             B.free(dst)
+
+        # one-sided atomics: every rank's fetch-adds on words of every member
+        NCNT, NOPS = 64, 3000
+        ctr, ctr32 = B.malloc(NCNT * 8), B.malloc(NCNT * 4)
+        B.memset(ctr, 0, NCNT * 8, team=LOCAL)
+        B.memset(ctr32, 0, NCNT * 4, team=LOCAL)
+        t.barrier()
+        all_ops = [np.random.default_rng(500 + r).integers(0, [P, NCNT], (NOPS, 2))
+                   for r in range(world)]
+        ops = all_ops[rank]
+        fetched = t.amo("fetch_add", "int64", ops[:, 0], ctr + ops[:, 1] * 8, np.ones(NOPS))
+        t.amo("add", "int32", ops[:, 0], ctr32 + ops[:, 1] * 4, np.full(NOPS, 3))
+        t.barrier()
+        hist = np.zeros((P, NCNT), np.int64)
+        for o in all_ops:
+            np.add.at(hist, (o[:, 0], o[:, 1]), 1)
+        ok = np.array_equal(B.get_rows(ctr, NCNT * 8, np.int64, team=LOCAL), hist[mine])
+        ok = ok and np.array_equal(B.get_rows(ctr32, NCNT * 4, np.int32, team=LOCAL),
+                                   3 * hist[mine])
+        fl = [None] * world
+        dist.all_gather_object(fl, fetched.tolist())
+        seen = {}
+        for r in range(world):
+            for (m, c), f in zip(all_ops[r].tolist(), fl[r]):
+                seen.setdefault((m, c), []).append(f)
+        ok = ok and all(sorted(v) == list(range(len(v))) for v in seen.values())
+        res.append(("amo", 0, bool(ok), ""))
+        try:  # a member outside the team: the caller's own call fails
+            t.amo("add", "int64", [P], [ctr], [1])
+            res.append(("amo_bad_member", 0, False, "not refused"))
+        except B.B200Error:
+            res.append(("amo_bad_member", 0, True, ""))
         t.close()
     except Exception as e:  # reported, then the group is left in order
         res.append(("error", -1, False, repr(e)))
@@ -158,7 +191,9 @@ def run_world(world):
 def test_peer_team_matches_oracle(world):
     """reduce (every dtype class, butterfly and other orders, several
     chunks), fcollect and alltoall (16-byte and byte paths) over world x 4
-    members, each rank's members checked against the oracle."""
+    members, each rank's members checked against the oracle; one-sided
+    atomics from every rank on every member: exact counts, and each
+    counter's fetched values a permutation of 0..count-1."""
     out = run_world(world)
     assert sorted(out) == list(range(world))
     for rank, res in out.items():
