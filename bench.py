@@ -379,11 +379,41 @@ def main():
         B.quiet()
         barrier()
         ems = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+        # the transfer bound: the same bytes in and out over PCIe with no
+        # reduction, the two directions on two streams at once
+        dev_in = {i: torch.empty(xs[i].shape, dtype=pinned_in[i].dtype, device="cuda")
+                  for i in used}
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def copy_step():
+            for _, _, _, _, _, i in calls:
+                with torch.cuda.stream(s_in):
+                    dev_in[i].copy_(pinned_in[i], non_blocking=True)
+                with torch.cuda.stream(s_out):
+                    pinned_out[i].copy_(dev_in[i], non_blocking=True)
+        copy_step()
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(s)
+        for st_ in (s_in, s_out):
+            st_.wait_event(c0)
+        for _ in range(args.e2e_steps):
+            copy_step()
+        for st_ in (s_in, s_out):
+            s.wait_stream(st_)
+        c1.record(s)
+        torch.cuda.synchronize()
+        cms = max_over_ranks(c0.elapsed_time(c1), dist, "cuda")
+        del dev_in
         e2e = {"value": round(job_gbs(step_bytes, args.e2e_steps, world, ems), 3),
                "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "steps": args.e2e_steps, "ms_per_step": round(ems / args.e2e_steps, 3),
                "path": "b200shm_reduce_host (pinned host rows in and out; copy in, reduce and "
-                       "copy out pipelined in chunks on three streams)"}
+                       "copy out pipelined in chunks on three streams)",
+               "transfer_bound": {"copy_only_ms_per_step": round(cms / args.e2e_steps, 3),
+                                  "frac": round(cms / ems, 4),
+                                  "what": "the same host->device and device->host bytes with no "
+                                          "reduction, both directions at once (pinned memory)"}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
