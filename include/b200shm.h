@@ -246,7 +246,9 @@ int64_t b200shm_barrier_flags_nonzero(void);
  * here another GPU's arena is one mapped address range. */
 int b200shm_ipc_handle(void *handle);
 /* Map another engine's arena from its IPC handle; *peer_base receives the
- * device address of its slice 0. */
+ * device address of its slice 0.  A handle opened again shares the first
+ * mapping (each open wants a close); b200shm_finalize closes the mappings
+ * still open. */
 int b200shm_peer_open(const void *handle, void **peer_base);
 int b200shm_peer_close(void *peer_base);
 
@@ -265,9 +267,10 @@ int b200shm_peer_close(void *peer_base);
 int b200shm_span_combine(int op, int dtype, int G, int rank, const uint64_t *partials,
                          int pe_start, int pe_stride, int pe_count, uint64_t dest_off,
                          uint64_t nelems, void *stream);
-/* fcollect over the same team: member m = g*pe_count + k (on GPU g) sends
- * nbytes from src_off; every local member's dest holds the G*pe_count
- * blocks in member order.  bases[g] = GPU g's arena base (this rank's own
+/* fcollect over the same team: member m = g*pe_count + k is PE
+ * pe_start + k*pe_stride of GPU g's engine (the same local PEs on every
+ * GPU) and sends nbytes from src_off; every local member's dest holds the
+ * G*pe_count blocks in member order.  bases[g] = GPU g's arena base (this rank's own
  * b200shm_heap_base, the others' mapped).  Replaces fcollect_helper_*
  * (src/shcoll/src/fcollect.c:32-484) for a team across GPUs. */
 int b200shm_span_fcollect(int G, int rank, const uint64_t *bases, int pe_start, int pe_stride,

@@ -103,6 +103,7 @@ int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int 
 /* The device allocator of the symmetric heap (heap.cu, heap_core.cuh). */
 int heap_setup(uint64_t slice);
 void heap_teardown();
+void span_teardown(); /* closes the peer mappings still open */
 int heap_alloc(uint64_t bytes, uint64_t align, uint64_t *off);
 int heap_release(uint64_t off);
 uint64_t heap_free_bytes();

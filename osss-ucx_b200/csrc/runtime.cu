@@ -196,6 +196,7 @@ int b200shm_finalize(void) {
   cudaFree(s.fix_list);
   cudaFree(s.fix_count);
   heap_teardown();
+  span_teardown();
   s = State();
   return B200SHM_OK;
 }

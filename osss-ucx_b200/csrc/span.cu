@@ -32,6 +32,9 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
+#include <string>
 #include <type_traits>
 
 #include "internal.cuh"
@@ -250,6 +253,21 @@ int combine_for(int op, bool vec, dim3 g, cudaStream_t s, const SpanPtrs &p, int
   return fail(B200SHM_ERR_UNSUPPORTED, "span_combine: op %d on this dtype", op);
 }
 
+/* the peers' arenas mapped in this process, by IPC handle: a handle opened
+ * twice shares one mapping (counted), and finalize closes what is left */
+struct PeerMap {
+  void *base;
+  int refs;
+};
+struct Peers {
+  std::mutex mu;
+  std::map<std::string, PeerMap> by_handle;
+};
+Peers &peers() {
+  static Peers p;
+  return p;
+}
+
 /* validation shared by the span entry points */
 int span_check(int G, int rank, const uint64_t *addrs, int pe_start, int pe_stride, int L) {
   if (G < 1 || G > kSpanMax || (G & (G - 1)))
@@ -262,6 +280,15 @@ int span_check(int G, int rank, const uint64_t *addrs, int pe_start, int pe_stri
 }
 
 }  // namespace
+
+/* at finalize: every peer mapping still open is closed */
+void span_teardown() {
+  std::lock_guard<std::mutex> lk(peers().mu);
+  for (auto &kv : peers().by_handle) (void)cudaIpcCloseMemHandle(kv.second.base);
+  peers().by_handle.clear();
+  (void)cudaGetLastError();
+}
+
 }  // namespace b200
 
 using namespace b200;
@@ -282,16 +309,34 @@ int b200shm_ipc_handle(void *handle) {
 int b200shm_peer_open(const void *handle, void **peer_base) {
   if (!st().up) return fail(B200SHM_ERR_STATE, "b200shm is not initialised");
   if (!handle || !peer_base) return fail(B200SHM_ERR_ARG, "peer_open: null argument");
+  std::lock_guard<std::mutex> lk(peers().mu);
+  std::string key((const char *)handle, sizeof(cudaIpcMemHandle_t));
+  auto it = peers().by_handle.find(key);
+  if (it != peers().by_handle.end()) { /* mapped already: share the mapping */
+    it->second.refs++;
+    *peer_base = it->second.base;
+    return B200SHM_OK;
+  }
   cudaIpcMemHandle_t h;
   memcpy(&h, handle, sizeof(h));
-  B200_CK(cudaIpcOpenMemHandle(peer_base, h, cudaIpcMemLazyEnablePeerAccess));
+  void *b = nullptr;
+  B200_CK(cudaIpcOpenMemHandle(&b, h, cudaIpcMemLazyEnablePeerAccess));
+  peers().by_handle[key] = PeerMap{b, 1};
+  *peer_base = b;
   return B200SHM_OK;
 }
 
 int b200shm_peer_close(void *peer_base) {
   if (!peer_base) return B200SHM_OK;
-  B200_CK(cudaIpcCloseMemHandle(peer_base));
-  return B200SHM_OK;
+  std::lock_guard<std::mutex> lk(peers().mu);
+  for (auto it = peers().by_handle.begin(); it != peers().by_handle.end(); ++it) {
+    if (it->second.base != peer_base) continue;
+    if (--it->second.refs > 0) return B200SHM_OK;
+    peers().by_handle.erase(it);
+    B200_CK(cudaIpcCloseMemHandle(peer_base));
+    return B200SHM_OK;
+  }
+  return fail(B200SHM_ERR_ARG, "peer_close: %p is not an open peer mapping", peer_base);
 }
 
 int b200shm_span_combine(int op, int dtype, int G, int rank, const uint64_t *partials,

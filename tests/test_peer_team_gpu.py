@@ -112,6 +112,23 @@ def _rank_main(rank, world, port, q):
             B.free(src)
             B.free(dst)
 
+        # a second team over the same engines shares the peer mappings; its
+        # reduction into a dest 4 bytes off 16-byte alignment takes the
+        # element-wise combine; closing it leaves the first team's mappings
+        t2 = spanning.PeerTeam(B, L, local_start=LOCAL[0], local_stride=LOCAL[1],
+                               scratch_bytes=1 << 16)
+        x = inputs("sum", "float32", P, 5001, 77)
+        nb = x[0].nbytes
+        src, dst = B.malloc(nb), B.malloc(nb + 16)
+        B.put_rows(src, x[mine], team=LOCAL)
+        assert t2.reduce("sum", "float32", "rec_dbl", dst + 4, src, 5001)
+        got = B.get_rows(dst + 4, nb, np.float32, team=LOCAL)
+        want = rs.reduce("rec_dbl", "sum", x)[mine]
+        res.append(("reduce_unaligned", 0, got.tobytes() == want.tobytes(), ""))
+        t2.close()
+        B.free(src)
+        B.free(dst)
+
         rng = np.random.default_rng(7 + world)
         for nb in (48, 4096, 3):
             x = rng.integers(0, 256, (P, P * nb), dtype=np.uint8)
