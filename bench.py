@@ -654,6 +654,20 @@ def run_movement(args, world, rank, local):
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f)
+    # the write bound of fcollect64, which writes P x P x N x 8 bytes and
+    # reads P x N x 8: the driver's memset of the same dest rows, timed alike
+    def memset_fc():
+        B.memset(fc_d, 0, PM * NF * 8, team=team, stream=s_ptr)
+    for _ in range(args.warmup):
+        memset_fc()
+    B.quiet()
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(st)
+    for _ in range(args.steps):
+        memset_fc()
+    w1.record(st)
+    B.quiet()
+    memset_ms = w0.elapsed_time(w1) / args.steps
     res = {}
     launches0 = B.launch_count()
     runs = args.warmup + args.steps
@@ -678,6 +692,11 @@ def run_movement(args, world, rank, local):
             res[name]["gbs_at_16B_per_op"] = round(units * 16 / (ms / 1e3) / 1e9, 1)
             res[name]["traffic"] = traffic.get(name)
     launches = B.launch_count() - launches0
+    res["fcollect64"]["write_bound"] = {
+        "memset_ms": round(memset_ms, 4),
+        "memset_gbs": round(PM * PM * NF * 8 / (memset_ms / 1e3) / 1e9, 1),
+        "frac": round(memset_ms / res["fcollect64"]["ms"], 4),
+        "what": "cudaMemset2DAsync of the same dest rows (writes only), against fcollect64's time"}
     # bit-exact checks of each op's last result against the oracle
     got = B.get_rows(a2a_d, PM * BLK, np.uint8, team=team)
     res["alltoallmem"]["bit_exact"] = got.tobytes() == rs.alltoall(x_a2a).tobytes()
