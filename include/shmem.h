@@ -49,6 +49,16 @@ enum { SHMEM_CMP_EQ = 0, SHMEM_CMP_NE, SHMEM_CMP_GT, SHMEM_CMP_LE, SHMEM_CMP_LT,
 #define SHMEM_THREAD_FUNNELED 1
 #define SHMEM_THREAD_SERIALIZED 2
 #define SHMEM_THREAD_MULTIPLE 3
+/* the specification this surface follows, and this library's own name */
+#define SHMEM_MAJOR_VERSION 1
+#define SHMEM_MINOR_VERSION 5
+#define SHMEM_MAX_NAME_LEN 64
+#define SHMEM_VENDOR_STRING "b200-shmem"
+#define SHMEM_VENDOR_MAJOR_VERSION 1
+#define SHMEM_VENDOR_MINOR_VERSION 0
+#define SHMEM_VENDOR_PATCH_VERSION 0
+#define SHMEM_MALLOC_ATOMICS_REMOTE 0
+#define SHMEM_MALLOC_SIGNAL_REMOTE 1
 
 typedef void *shmem_team_t;
 typedef void *shmem_ctx_t;
@@ -113,7 +123,38 @@ void shmem_barrier_all(void);
 void shmem_sync_all(void);
 void shmem_barrier(int PE_start, int logPE_stride, int PE_size, long *pSync);
 void shmem_sync(int PE_start, int logPE_stride, int PE_size, long *pSync);
+/* the active-set form under the name the reference exports for it */
+void shmem_sync_deprecated(int PE_start, int logPE_stride, int PE_size, long *pSync);
 int shmem_team_sync(shmem_team_t team);
+#if !defined(SHMEM_B200_NO_GENERICS)
+/* shmem_sync(team) and shmem_sync(PE_start, logPE_stride, PE_size, pSync),
+ * told apart by their number of arguments */
+#define SHMEM_B200_SYNC_PICK(a, b, c, d, f, ...) f
+#define SHMEM_B200_SYNC_4(s, l, n, p) shmem_sync_deprecated(s, l, n, p)
+#define SHMEM_B200_SYNC_1(team) shmem_team_sync(team)
+#define shmem_sync(...)                                                        \
+  SHMEM_B200_SYNC_PICK(__VA_ARGS__, SHMEM_B200_SYNC_4, SHMEM_B200_SYNC_4,      \
+                       SHMEM_B200_SYNC_4, SHMEM_B200_SYNC_1, 0)(__VA_ARGS__)
+#endif
+
+/* ---- locks (src/api/lock.c): a symmetric long, 0 when free -------------- */
+void shmem_set_lock(long *lock);
+int shmem_test_lock(long *lock);
+void shmem_clear_lock(long *lock);
+
+/* ---- library state and information (src/api/{init,info,tl_query}.c) ---- */
+int shmem_initialized(void);
+int shmem_finalized(void);
+void shmem_query_thread(int *provided);
+void shmem_info_get_version(int *major, int *minor);
+void shmem_info_get_name(char *name);
+void shmem_info_get_version_number(int *version);
+void shmem_info_get_vendor_version(int *major, int *minor, int *patch);
+void shmem_info_get_vendor_version_number(int *version);
+void shmem_pcontrol(const int level, ...);
+int shmem_addr_accessible(const void *addr, int pe);
+void *shmem_realloc(void *ptr, size_t size);
+void *shmem_malloc_with_hints(size_t size, long hints);
 
 /* ---- teams (include/shmem/teams.h) -------------------------------------- */
 int shmem_team_my_pe(shmem_team_t team);
@@ -514,6 +555,30 @@ uint64_t shmem_signal_wait_until(uint64_t *sig_addr, int cmp, uint64_t cmp_value
                                               _type *cmp_values);
 SHMEM_B200_SYNC_TYPES(SHMEM_B200_DECL_SYNC_ONE)
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_SYNC_VEC)
+
+/* ---- the atomics' names before OpenSHMEM 1.4 (api.h, deprecated) -------- */
+#define SHMEM_B200_DECL_AMO_OLD(_type, _tn)                                     \
+  _type shmem_##_tn##_fadd(_type *target, _type value, int pe);                \
+  _type shmem_##_tn##_finc(_type *target, int pe);                             \
+  void shmem_##_tn##_add(_type *target, _type value, int pe);                  \
+  void shmem_##_tn##_inc(_type *target, int pe);                               \
+  _type shmem_##_tn##_cswap(_type *target, _type cond, _type value, int pe);   \
+  _type shmem_##_tn##_swap(_type *target, _type value, int pe);                \
+  _type shmem_##_tn##_fetch(const _type *target, int pe);                      \
+  void shmem_##_tn##_set(_type *target, _type value, int pe);
+#define SHMEM_B200_DECL_AMO_OLD_EXT(_type, _tn)                                 \
+  _type shmem_##_tn##_swap(_type *target, _type value, int pe);                \
+  _type shmem_##_tn##_fetch(const _type *target, int pe);                      \
+  void shmem_##_tn##_set(_type *target, _type value, int pe);
+#define SHMEM_B200_AMO_OLD_TYPES(X) X(int, int) X(long, long) X(long long, longlong)
+#define SHMEM_B200_AMO_OLD_EXT_TYPES(X) X(float, float) X(double, double)
+SHMEM_B200_AMO_OLD_TYPES(SHMEM_B200_DECL_AMO_OLD)
+SHMEM_B200_AMO_OLD_EXT_TYPES(SHMEM_B200_DECL_AMO_OLD_EXT)
+
+#if !defined(__cplusplus) && defined(__STDC_VERSION__) && __STDC_VERSION__ >= 201112L && \
+    !defined(SHMEM_B200_NO_GENERICS)
+#include "shmem_generics.h"
+#endif
 
 #ifdef __cplusplus
 }

@@ -33,9 +33,57 @@
 #include <string.h>
 #include <time.h>
 
+/* the library defines the functions themselves: no generic-name macros */
+#define SHMEM_B200_NO_GENERICS 1
 #include "../../include/b200shm.h"
 #include "../../include/shmem.h"
 #include "../../include/shmemx.h"
+
+/* ---- sizes of the live symmetric objects (for shmem_realloc) --------------- */
+static pthread_mutex_t g_sz_mu = PTHREAD_MUTEX_INITIALIZER;
+static uint64_t *g_sz_off, *g_sz_len;
+static size_t g_sz_n, g_sz_cap;
+
+static void size_note(uint64_t off, uint64_t len) {
+  pthread_mutex_lock(&g_sz_mu);
+  if (g_sz_n == g_sz_cap) {
+    const size_t cap = g_sz_cap ? 2 * g_sz_cap : 64;
+    uint64_t *o = (uint64_t *)realloc(g_sz_off, cap * sizeof(uint64_t));
+    if (o) g_sz_off = o;
+    uint64_t *l = (uint64_t *)realloc(g_sz_len, cap * sizeof(uint64_t));
+    if (l) g_sz_len = l;
+    if (o && l) g_sz_cap = cap;
+  }
+  if (g_sz_n < g_sz_cap) {
+    g_sz_off[g_sz_n] = off;
+    g_sz_len[g_sz_n] = len;
+    g_sz_n++;
+  }
+  pthread_mutex_unlock(&g_sz_mu);
+}
+static void size_forget(uint64_t off) {
+  pthread_mutex_lock(&g_sz_mu);
+  for (size_t i = 0; i < g_sz_n; i++)
+    if (g_sz_off[i] == off) {
+      g_sz_off[i] = g_sz_off[g_sz_n - 1];
+      g_sz_len[i] = g_sz_len[g_sz_n - 1];
+      g_sz_n--;
+      break;
+    }
+  pthread_mutex_unlock(&g_sz_mu);
+}
+/* bytes of the object at `off`; 0 if none starts there */
+static uint64_t size_of_object(uint64_t off) {
+  uint64_t len = 0;
+  pthread_mutex_lock(&g_sz_mu);
+  for (size_t i = 0; i < g_sz_n; i++)
+    if (g_sz_off[i] == off) {
+      len = g_sz_len[i];
+      break;
+    }
+  pthread_mutex_unlock(&g_sz_mu);
+  return len;
+}
 
 /* ---- errors ---------------------------------------------------------------- */
 static __thread char t_err[512];
@@ -265,9 +313,12 @@ static int launch(b200_team_t *t, agg_t *g) {
     uint64_t off = 0;
     int rc = b200shm_malloc(r->n, r->a, &off);
     g->out = off;
+    if (rc == 0) size_note(off, r->n);
     return engine_err(rc);
   }
-  case K_FREE: return engine_err(b200shm_free(r->dest));
+  case K_FREE:
+    size_forget(r->dest);
+    return engine_err(b200shm_free(r->dest));
   case K_BARRIER: return engine_err(b200shm_barrier(r->algo, t->start, t->stride, t->size, NULL));
   case K_REDUCE:
     return engine_err(b200shm_reduce(r->op, r->dtype, r->algo, t->start, t->stride, t->size,
@@ -406,16 +457,52 @@ int shmemx_b200_run(int npes, void (*pe_main)(void *), void *arg) {
 }
 
 /* ---- setup / query ----------------------------------------------------------- */
+static __thread int t_finalized;
+static int g_thread_level = SHMEM_THREAD_SINGLE;
 void shmem_init(void) {
   if (t_pe >= 0) return; /* PE threads are set up by shmemx_b200_run */
   if (engine_up(1) == 0) t_pe = 0; /* a lone thread becomes a 1-PE job */
 }
 int shmem_init_thread(int requested, int *provided) {
   shmem_init();
-  if (provided) *provided = requested;
+  if (requested >= SHMEM_THREAD_SINGLE && requested <= SHMEM_THREAD_MULTIPLE)
+    g_thread_level = requested; /* every level is provided */
+  if (provided) *provided = g_thread_level;
   return t_pe >= 0 ? 0 : -1;
 }
-void shmem_finalize(void) { shmem_barrier_all(); }
+void shmem_finalize(void) {
+  shmem_barrier_all();
+  t_finalized = 1;
+}
+int shmem_initialized(void) { return t_pe >= 0 && !t_finalized; }
+int shmem_finalized(void) { return t_finalized; }
+void shmem_query_thread(int *provided) {
+  if (provided) *provided = g_thread_level;
+}
+void shmem_info_get_version(int *major, int *minor) {
+  if (major) *major = SHMEM_MAJOR_VERSION;
+  if (minor) *minor = SHMEM_MINOR_VERSION;
+}
+void shmem_info_get_name(char *name) {
+  if (!name) return;
+  strncpy(name, SHMEM_VENDOR_STRING, SHMEM_MAX_NAME_LEN - 1);
+  name[SHMEM_MAX_NAME_LEN - 1] = '\0';
+}
+/* major * 100 + minor, and that * 100 + patch for the vendor's */
+void shmem_info_get_version_number(int *version) {
+  if (version) *version = SHMEM_MAJOR_VERSION * 100 + SHMEM_MINOR_VERSION;
+}
+void shmem_info_get_vendor_version(int *major, int *minor, int *patch) {
+  if (major) *major = SHMEM_VENDOR_MAJOR_VERSION;
+  if (minor) *minor = SHMEM_VENDOR_MINOR_VERSION;
+  if (patch) *patch = SHMEM_VENDOR_PATCH_VERSION;
+}
+void shmem_info_get_vendor_version_number(int *version) {
+  if (version)
+    *version = (SHMEM_VENDOR_MAJOR_VERSION * 100 + SHMEM_VENDOR_MINOR_VERSION) * 100 +
+               SHMEM_VENDOR_PATCH_VERSION;
+}
+void shmem_pcontrol(const int level, ...) { (void)level; /* no profiling levels */ }
 int shmem_my_pe(void) { return t_pe; }
 int shmem_n_pes(void) { return g_npes; }
 int shmem_pe_accessible(int pe) { return pe >= 0 && pe < g_npes; }
@@ -446,6 +533,35 @@ void shmem_free(void *ptr) {
   r.kind = K_FREE;
   if (sym_off(ptr, &r.dest)) return;
   arrive(&g_world, &r);
+}
+void *shmem_malloc_with_hints(size_t size, long hints) {
+  (void)hints; /* every object is reachable by atomics and signals alike */
+  return shmem_malloc(size);
+}
+/* Collective, like shmem_malloc: a new object of `size` bytes, this PE's
+ * first min(old, new) bytes copied into it, the old object freed. */
+void *shmem_realloc(void *ptr, size_t size) {
+  if (!ptr) return shmem_malloc(size);
+  uint64_t off = 0;
+  if (sym_off(ptr, &off)) {
+    t_status = set_err(B200SHM_ERR_ARG, "shmem_realloc: %p is not a symmetric object", ptr);
+    return NULL;
+  }
+  if (size == 0) {
+    shmem_free(ptr);
+    return NULL;
+  }
+  const uint64_t old = size_of_object(off);
+  char *p = (char *)shmem_malloc(size);
+  if (!p) return NULL; /* the old object stays */
+  const uint64_t keep = old < size ? old : size;
+  if (keep) t_status = engine_err(b200shm_memcpy(p, ptr, keep, NULL));
+  shmem_free(ptr); /* collective: every member's copy is done before it returns */
+  return p;
+}
+int shmem_addr_accessible(const void *addr, int pe) {
+  uint64_t off = 0;
+  return sym_off(addr, &off) == 0 && pe >= 0 && pe < g_npes;
 }
 void *shmem_ptr(const void *dest, int pe) {
   uint64_t off = 0;
@@ -795,6 +911,9 @@ void shmem_barrier(int PE_start, int logPE_stride, int PE_size, long *pSync) {
 void shmem_sync(int PE_start, int logPE_stride, int PE_size, long *pSync) {
   (void)pSync;
   barrier_on(active_set(PE_start, logPE_stride, PE_size), g_sync_algo);
+}
+void shmem_sync_deprecated(int PE_start, int logPE_stride, int PE_size, long *pSync) {
+  shmem_sync(PE_start, logPE_stride, PE_size, pSync);
 }
 int shmem_team_sync(shmem_team_t team) {
   return barrier_on((b200_team_t *)team, g_team_sync_algo);
@@ -1652,3 +1771,77 @@ uint64_t shmem_signal_wait_until(uint64_t *sig_addr, int cmp, uint64_t cmp_value
   wait_pass(W_ONE, cmp, B200SHM_U64, sig_addr, 1, NULL, &cmp_value, NULL, NULL, &seen, &p);
   return seen;
 }
+
+/* ---- locks (src/api/lock.c) ---------------------------------------------------
+ * A lock is a symmetric long, 0 when free.  Its word on one owner PE (spread
+ * over the PEs by the lock's offset) holds 0 or the holder's PE + 1, and
+ * changes only by compare-and-swap through the engine's atomics.  set_lock
+ * retries until its swap wins, yielding the thread between tries; test_lock
+ * tries once; clear_lock completes the holder's outstanding puts first
+ * (shmem_quiet), then swaps its PE + 1 back to 0. */
+static long *lock_word(long *lock, int *owner) {
+  uint64_t off = 0;
+  if (sym_off(lock, &off)) {
+    t_status = set_err(B200SHM_ERR_ARG, "lock %p is not a symmetric object", (void *)lock);
+    return NULL;
+  }
+  *owner = (int)((off >> 3) % (uint64_t)g_npes);
+  return lock;
+}
+static int lock_try(long *lock) {
+  int owner = 0;
+  long *w = lock_word(lock, &owner);
+  if (!w) return -1;
+  const long old = shmem_long_atomic_compare_swap(w, 0, (long)t_pe + 1, owner);
+  if (t_status) return -1;
+  return old == 0;
+}
+void shmem_set_lock(long *lock) {
+  for (;;) {
+    const int got = lock_try(lock);
+    if (got != 0) return; /* taken, or an error left in t_status */
+    sched_yield();
+  }
+}
+int shmem_test_lock(long *lock) {
+  const int got = lock_try(lock);
+  return got == 1 ? 0 : 1; /* 0: the lock is now this PE's */
+}
+void shmem_clear_lock(long *lock) {
+  int owner = 0;
+  long *w = lock_word(lock, &owner);
+  if (!w) return;
+  shmem_quiet();
+  const long old = shmem_long_atomic_compare_swap(w, (long)t_pe + 1, 0, owner);
+  if (!t_status && old != (long)t_pe + 1)
+    t_status = set_err(B200SHM_ERR_STATE, "shmem_clear_lock: PE %d does not hold the lock", t_pe);
+}
+
+/* ---- the atomics' names before OpenSHMEM 1.4 ------------------------------------ */
+#define DEF_AMO_OLD(_type, _tn)                                                \
+  _type shmem_##_tn##_fadd(_type *target, _type value, int pe) {               \
+    return shmem_##_tn##_atomic_fetch_add(target, value, pe);                  \
+  }                                                                            \
+  _type shmem_##_tn##_finc(_type *target, int pe) {                            \
+    return shmem_##_tn##_atomic_fetch_inc(target, pe);                         \
+  }                                                                            \
+  void shmem_##_tn##_add(_type *target, _type value, int pe) {                 \
+    shmem_##_tn##_atomic_add(target, value, pe);                               \
+  }                                                                            \
+  void shmem_##_tn##_inc(_type *target, int pe) { shmem_##_tn##_atomic_inc(target, pe); } \
+  _type shmem_##_tn##_cswap(_type *target, _type cond, _type value, int pe) {  \
+    return shmem_##_tn##_atomic_compare_swap(target, cond, value, pe);         \
+  }
+#define DEF_AMO_OLD_EXT(_type, _tn)                                            \
+  _type shmem_##_tn##_swap(_type *target, _type value, int pe) {               \
+    return shmem_##_tn##_atomic_swap(target, value, pe);                       \
+  }                                                                            \
+  _type shmem_##_tn##_fetch(const _type *target, int pe) {                     \
+    return shmem_##_tn##_atomic_fetch(target, pe);                             \
+  }                                                                            \
+  void shmem_##_tn##_set(_type *target, _type value, int pe) {                 \
+    shmem_##_tn##_atomic_set(target, value, pe);                               \
+  }
+SHMEM_B200_AMO_OLD_TYPES(DEF_AMO_OLD)
+SHMEM_B200_AMO_OLD_TYPES(DEF_AMO_OLD_EXT)
+SHMEM_B200_AMO_OLD_EXT_TYPES(DEF_AMO_OLD_EXT)

@@ -257,3 +257,45 @@ def test_peer_team_host_logic_two_ranks():
 
 def test_peer_team_host_logic_four_ranks():
     check(4)
+
+
+def _odd_world_main(rank, world, port, tag, q):
+    import datetime
+    import torch.distributed as dist
+    for p in (os.path.join(ROOT, "osss-ucx_b200"), os.path.join(ROOT, "oracle"),
+              os.path.join(ROOT, "tests")):
+        sys.path.insert(0, p)
+    import oracle
+    import spanning
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    eng = ShmEngine("b200peer%s_%d" % (tag, rank), rank, oracle.Restatement())
+    try:
+        spanning.PeerTeam(eng, L, local_start=LOCAL[0], local_stride=LOCAL[1],
+                          scratch_bytes=4096)
+        out = "accepted"
+    except ValueError:
+        out = "refused"
+    dist.barrier()
+    eng.close()
+    dist.destroy_process_group()
+    q.put((rank, out))
+
+
+def test_peer_team_refuses_a_world_that_is_not_a_power_of_two():
+    """Three ranks: the butterfly over GPUs needs a power of two, and every
+    rank refuses alike (before any mapping is made)."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    tag = "%d_%d" % (os.getpid(), port)
+    ps = [ctx.Process(target=_odd_world_main, args=(r, 3, port, tag, q)) for r in range(3)]
+    for p in ps:
+        p.start()
+    out = dict(q.get(timeout=300) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out == {0: "refused", 1: "refused", 2: "refused"}

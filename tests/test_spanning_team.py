@@ -143,7 +143,9 @@ def test_engine_steps_on_one_gpu(B, heap, rs):
     viewed in place as a tensor, and the write-back broadcasts it to every
     local member -- the same bits as b200shm_reduce over those members;
     fcollect and alltoall through the engine's local steps, and atomics
-    through the routing, give the oracle's bytes and counts."""
+    through the routing, give the oracle's bytes and counts.  The
+    peer-memory form (PeerTeam) in the same world: G = 1, the span kernels
+    over this GPU's arena alone, barriers through NCCL."""
     import datetime
     import torch.distributed as dist
     sys.path.insert(0, os.path.join(ROOT, "osss-ucx_b200"))
@@ -187,6 +189,29 @@ def test_engine_steps_on_one_gpu(B, heap, rs):
         for (m, c), f in zip(ops.tolist(), fetched.tolist()):
             seen.setdefault((m, c), []).append(f)
         assert all(sorted(v) == list(range(len(v))) for v in seen.values())
+
+        # the peer-memory form in the same world of one: G = 1, its own arena
+        # only, barriers through NCCL
+        P8, team8 = 8, (7, 2, 8)
+        pt = spanning.PeerTeam(B, P8, local_start=7, local_stride=2, scratch_bytes=1 << 14)
+        x = inputs("sum", "float32", P8, P8)
+        src, dst = heap(x[0].nbytes), heap(x[0].nbytes)
+        B.put_rows(src, x, team=team8)
+        assert pt.reduce("sum", "float32", "rec_dbl", dst, src, N)
+        assert B.get_rows(dst, x[0].nbytes, x.dtype, team=team8).tobytes() == \
+            rs.reduce("rec_dbl", "sum", x).tobytes()
+        xb = np.random.default_rng(5).integers(0, 256, (P8, P8 * nb), dtype=np.uint8)
+        B.put_rows(src, xb, team=team8)
+        pt.fcollect(dst, src, nb)
+        want = rs.fcollect(np.ascontiguousarray(xb[:, :nb]))
+        assert B.get_rows(dst, P8 * nb, np.uint8, team=team8).tobytes() == want.tobytes()
+        pt.alltoall(dst, src, nb)
+        assert B.get_rows(dst, P8 * nb, np.uint8, team=team8).tobytes() == \
+            rs.alltoall(xb).tobytes()
+        B.memset(ctr, 0, 64 * 8, team=team)  # members 0..5 of team8 are team's
+        fetched = pt.amo("fetch_add", "int64", ops[:, 0], ctr + ops[:, 1] * 8, np.ones(500))
+        assert np.array_equal(B.get_rows(ctr, 64 * 8, np.int64, team=team), hist)
+        pt.close()
     finally:
         dist.destroy_process_group()
 

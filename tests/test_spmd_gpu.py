@@ -244,3 +244,53 @@ def test_spmd_point_to_point_sync_and_signalled_puts(tmp_path):
                                        SHMEM_B200_WAIT_TIMEOUT="60"),
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+def compile_generics(tmp_path):
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_generics")
+    subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Wextra", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_generics.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    return exe
+
+
+def test_generic_names_resolve_to_the_typed_functions(tmp_path):
+    """The C11 generic names compile (C11, every warning an error) and link
+    in a program that uses them on a dozen types, with and without a
+    context first; the sized typedefs select the functions of the types
+    they alias; a generic call on a type outside its table does not
+    compile."""
+    assert os.path.exists(compile_generics(tmp_path))
+    inc = "-I" + os.path.join(ROOT, "include")
+    good = tmp_path / "good.c"
+    good.write_text(
+        '#include <stdint.h>\n#include "shmem.h"\n'
+        "int64_t f(int64_t *c, uint32_t *u, size_t *s, int8_t *d, const int8_t *x) {\n"
+        "  shmem_atomic_fetch_and(u, 3u, 0);\n"
+        "  shmem_atomic_add(s, (size_t)1, 0);\n"
+        "  shmem_and_reduce(SHMEM_TEAM_WORLD, d, x, 4);\n"
+        "  return shmem_atomic_fetch_add(c, (int64_t)1, 0);\n}\n")
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-fsyntax-only", inc, str(good)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    bad = tmp_path / "bad.c"
+    bad.write_text('#include "shmem.h"\n'
+                   "float f(float *p) { return shmem_atomic_fetch_add(p, 1.0f, 0); }\n")
+    r = subprocess.run(["gcc", "-std=c11", "-fsyntax-only", inc, str(bad)],
+                       capture_output=True, text=True)
+    assert r.returncode != 0 and "b200_shmem_generic_type_error" in r.stderr, r.stderr
+
+
+@pytest.mark.gpu
+def test_spmd_generics_program(tmp_path):
+    """tests/c/spmd_generics.c checks itself: generic RMA, atomics (and the
+    pre-1.4 names), reductions, collectives and waits; locks around a
+    read-modify-write; realloc; the version, name and state queries."""
+    exe = compile_generics(tmp_path)
+    r = subprocess.run([exe], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M",
+                                       SHMEM_B200_WAIT_TIMEOUT="60"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
