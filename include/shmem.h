@@ -155,6 +155,24 @@ void shmem_pcontrol(const int level, ...);
 int shmem_addr_accessible(const void *addr, int pe);
 void *shmem_realloc(void *ptr, size_t size);
 void *shmem_malloc_with_hints(size_t size, long hints);
+/* the address of `dest` on team member `pe`, NULL when not reachable */
+void *shmem_team_ptr(shmem_team_t team, const void *dest, int pe);
+
+/* ---- names before OpenSHMEM 1.2 and the cache routines (api.h, cache.h) -- */
+void start_pes(int npes);
+int _my_pe(void);
+int _num_pes(void);
+void *shmalloc(size_t size);
+void shfree(void *ptr);
+void *shrealloc(void *ptr, size_t size);
+void *shmemalign(size_t alignment, size_t size);
+/* no cache to manage: these do nothing */
+void shmem_set_cache_inv(void);
+void shmem_set_cache_line_inv(void *dest);
+void shmem_clear_cache_inv(void);
+void shmem_clear_cache_line_inv(void *dest);
+void shmem_udcflush(void);
+void shmem_udcflush_line(void *dest);
 
 /* ---- teams (include/shmem/teams.h) -------------------------------------- */
 int shmem_team_my_pe(shmem_team_t team);

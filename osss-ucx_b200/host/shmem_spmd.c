@@ -559,6 +559,28 @@ void *shmem_realloc(void *ptr, size_t size) {
   shmem_free(ptr); /* collective: every member's copy is done before it returns */
   return p;
 }
+void *shmem_team_ptr(shmem_team_t team, const void *dest, int pe) {
+  const b200_team_t *t = (const b200_team_t *)team;
+  if (!t || !t->valid || pe < 0 || pe >= t->size) return NULL;
+  return shmem_ptr(dest, t->start + pe * t->stride);
+}
+/* names before OpenSHMEM 1.2 */
+void start_pes(int npes) {
+  (void)npes; /* the job's size is shmemx_b200_run's */
+  shmem_init();
+}
+int _my_pe(void) { return shmem_my_pe(); }
+int _num_pes(void) { return shmem_n_pes(); }
+void *shmalloc(size_t size) { return shmem_malloc(size); }
+void shfree(void *ptr) { shmem_free(ptr); }
+void *shrealloc(void *ptr, size_t size) { return shmem_realloc(ptr, size); }
+void *shmemalign(size_t alignment, size_t size) { return shmem_align(alignment, size); }
+void shmem_set_cache_inv(void) {}
+void shmem_set_cache_line_inv(void *dest) { (void)dest; }
+void shmem_clear_cache_inv(void) {}
+void shmem_clear_cache_line_inv(void *dest) { (void)dest; }
+void shmem_udcflush(void) {}
+void shmem_udcflush_line(void *dest) { (void)dest; }
 int shmem_addr_accessible(const void *addr, int pe) {
   uint64_t off = 0;
   return sym_off(addr, &off) == 0 && pe >= 0 && pe < g_npes;

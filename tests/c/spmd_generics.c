@@ -16,8 +16,9 @@
  *  - shmem_wait_until / shmem_test on a flag another PE puts;
  *  - shmem_set_lock / shmem_clear_lock around a read-modify-write of a
  *    counter on PE 0 (every increment survives), shmem_test_lock;
- *  - shmem_realloc keeps the first bytes, shmem_addr_accessible, the
- *    version and name queries, shmem_initialized / shmem_finalized.
+ *  - shmem_realloc keeps the first bytes, shmem_addr_accessible,
+ *    shmem_team_ptr, the pre-1.2 names, the version and name queries,
+ *    shmem_initialized / shmem_finalized.
  */
 #include <stdint.h>
 #include <stdio.h>
@@ -220,6 +221,11 @@ static void pe_main(void *arg) {
   if (r2)
     for (int i = 0; i < 16; i++) CHECK(r2[i] == me * 100 + i, "realloc kept [%d]", i);
   CHECK(shmem_addr_accessible(r2, next) == 1, "addr_accessible symmetric");
+  CHECK(shmem_team_ptr(SHMEM_TEAM_WORLD, r2, next) == shmem_ptr(r2, next), "team_ptr");
+  CHECK(_my_pe() == me && _num_pes() == NP, "pre-1.2 _my_pe / _num_pes");
+  long *old_style = shmalloc(8 * sizeof(long));
+  CHECK(old_style != NULL, "shmalloc");
+  shfree(old_style);
   CHECK(shmem_addr_accessible(isrc, next) == 0, "addr_accessible stack");
   int maj = 0, min = 0, ver = 0;
   char name[SHMEM_MAX_NAME_LEN];
