@@ -427,7 +427,13 @@ SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_BIT)
                                              _type *dest, _type value, int pe); \
   void shmem_ctx_##_tn##_atomic_fetch_xor_nbi(shmem_ctx_t ctx, _type *fetch,   \
                                               _type *dest, _type value,         \
-                                              int pe);
+                                              int pe);                          \
+  /* declared by the reference's api.h with the fetching signature: the same \
+   * operation as atomic_fetch_xor_nbi */                                       \
+  void shmem_##_tn##_atomic_xor_nbi(_type *fetch, _type *dest, _type value,    \
+                                    int pe);                                    \
+  void shmem_ctx_##_tn##_atomic_xor_nbi(shmem_ctx_t ctx, _type *fetch,         \
+                                        _type *dest, _type value, int pe);
 SHMEM_B200_AMO_STANDARD_TYPES(SHMEM_B200_DECL_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(SHMEM_B200_DECL_AMO_NBI_EXT)
 SHMEM_B200_AMO_BITWISE_TYPES(SHMEM_B200_DECL_AMO_NBI_BIT)

@@ -1405,6 +1405,15 @@ SHMEM_B200_AMO_BITWISE_TYPES(DEF_AMO_BIT)
                                           _type value, int pe) {               \
     shmem_ctx_##_tn##_atomic_fetch_xor_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
                                            value, pe);                         \
+  }                                                                            \
+  void shmem_ctx_##_tn##_atomic_xor_nbi(shmem_ctx_t ctx, _type *fetch,         \
+                                        _type *dest, _type value, int pe) {    \
+    shmem_ctx_##_tn##_atomic_fetch_xor_nbi(ctx, fetch, dest, value, pe);       \
+  }                                                                            \
+  void shmem_##_tn##_atomic_xor_nbi(_type *fetch, _type *dest, _type value,    \
+                                    int pe) {                                  \
+    shmem_ctx_##_tn##_atomic_fetch_xor_nbi(SHMEM_CTX_DEFAULT, fetch, dest,     \
+                                           value, pe);                         \
   }
 SHMEM_B200_AMO_STANDARD_TYPES(DEF_AMO_NBI_STD)
 SHMEM_B200_AMO_EXTENDED_TYPES(DEF_AMO_NBI_EXT)
