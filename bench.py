@@ -485,6 +485,44 @@ def config1_cpu_reference(reps=300):
                       "(pinned pthreads); median of %d calls between host barriers" % reps}
 
 
+def launch_floor_us(reps=300):
+    """The platform's floor under any blocking GPU call: one launch of an
+    empty kernel and a stream synchronisation, through the CUDA driver API
+    from ctypes (the way the C entry points are timed).  The kernel is a
+    one-instruction PTX entry loaded with cuModuleLoadData."""
+    import ctypes
+    import torch
+    torch.cuda.init()
+    torch.zeros(1, device="cuda")  # the primary context is current
+    cu = ctypes.CDLL("libcuda.so.1")
+    ptx = (b".version 8.0\n.target sm_90\n.address_size 64\n"
+           b".visible .entry b200_empty()\n{\n\tret;\n}\n\0")
+    mod, fn, strm = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    if cu.cuModuleLoadData(ctypes.byref(mod), ctypes.c_char_p(ptx)) != 0:
+        return None
+    if cu.cuModuleGetFunction(ctypes.byref(fn), mod, b"b200_empty") != 0:
+        return None
+    if cu.cuStreamCreate(ctypes.byref(strm), 1) != 0:
+        return None
+    launch, sync = cu.cuLaunchKernel, cu.cuStreamSynchronize
+    launch.argtypes = [ctypes.c_void_p] + [ctypes.c_uint] * 7 + [ctypes.c_void_p] * 3
+    sync.argtypes = [ctypes.c_void_p]
+
+    def one():
+        launch(fn, 1, 1, 1, 32, 1, 1, 0, strm, None, None)
+        sync(strm)
+    for _ in range(20):
+        one()
+    t = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        one()
+        t.append(time.perf_counter() - t0)
+    cu.cuStreamDestroy_v2(strm)
+    cu.cuModuleUnload(mod)
+    return round(float(np.median(t)) * 1e6, 2)
+
+
 def run_config1(args, world, rank, local, reps=300):
     """The reference's CPU-runnable configuration on the GPU: 8 PEs, team
     WORLD, int32 sum_reduce of 1024 elements (rec_dbl, the default), then
@@ -546,7 +584,11 @@ def run_config1(args, world, rank, local, reps=300):
 
         gpu = {"int32_sum_reduce_us": med_us(red), "fcollect64_us": med_us(fcol),
                "barrier_all_us": med_us(bar), "sequence_blocking_us": med_us(seq),
-               "sequence_stream_ordered_us": med_us(seq_ordered)}
+               "sequence_stream_ordered_us": med_us(seq_ordered),
+               "launch_sync_floor_us": launch_floor_us(reps),
+               "floor_what": "an empty kernel launched and its stream synchronised (CUDA "
+                             "driver API through ctypes): the least any blocking GPU call "
+                             "costs on this host"}
         red(), fcol()
         z = np.load(os.path.join(ROOT, "tests", "golden", "config1.npz"))
         exact = (B.get_rows(dst, 4096, np.int32, team=team).tobytes() == z["reduce_out"].tobytes()

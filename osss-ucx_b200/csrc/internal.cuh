@@ -34,7 +34,10 @@ struct State {
    * indices whose result depends on operand order; scratch owned by the
    * library, shared by all calls (calls that overlap on the GPU race) */
   unsigned long long *fix_list = nullptr;
-  unsigned long long *fix_count = nullptr;
+  unsigned long long *fix_count = nullptr; /* the batch path's count (zeroed per run) */
+  /* the per-call path's count and the replay kernel's exit counter: the
+   * replay's last CTA sets both back to zero, so they start every call at 0 */
+  unsigned long long *call_fix = nullptr;
   uint64_t fix_cap = 0;
 };
 

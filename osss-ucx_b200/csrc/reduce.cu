@@ -48,15 +48,23 @@ namespace {
 /* Second pass over the elements the streaming kernel deferred (it left
  * their dests untouched, so in-place sources are still intact): one CTA
  * per element stages the P inputs in shared memory, then replays the
- * algorithm's operand order from there. */
+ * algorithm's operand order from there.  Launched as a programmatic
+ * dependent of the streaming kernel: its CTAs may become resident during
+ * that kernel's last wave and wait here until its results are visible.
+ * The last CTA to leave sets the counter back to zero for the next call
+ * (every CTA reads it before it counts itself out), so no memset precedes
+ * the streaming kernel. */
 template <class T, int OP>
 __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
                                                     const unsigned long long *list,
-                                                    const unsigned long long *count,
+                                                    unsigned long long *count,
+                                                    unsigned long long *done,
                                                     unsigned long long cap) {
   __shared__ T vals[kFixMaxMembers];
   __shared__ T common;
-  const unsigned long long n = *count < cap ? *count : cap;
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const unsigned long long cnt = *(volatile unsigned long long *)count;
+  const unsigned long long n = cnt < cap ? cnt : cap;
   for (unsigned long long k = blockIdx.x; k < n; k += gridDim.x) {
     const uint64_t e = list[k];
     for (int j = threadIdx.x; j < a.P; j += blockDim.x)
@@ -88,12 +96,28 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
     }
     __syncthreads();
   }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(done, 1ull) == (unsigned long long)gridDim.x - 1) {
+      *(volatile unsigned long long *)count = 0;
+      *(volatile unsigned long long *)done = 0;
+      __threadfence();
+    }
+  }
+}
+
+/* Let the replay kernel that follows a MIN/MAX-checking launch be
+ * scheduled once every CTA of this grid has started (it waits for this
+ * grid's results before it reads anything). */
+__device__ __forceinline__ void allow_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 /* ---- the streaming kernels -------------------------------------------- */
 template <class T, int OP, int ORDER, int V, int U, bool MINMAX_CHECK, int LV>
 __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
   typedef Pack<T, V> PK;
+  if constexpr (MINMAX_CHECK) allow_dependents();
   /* grid-stride: all CTAs sweep one contiguous front of every member's
    * slice together, which keeps DRAM row locality (contiguous per-CTA
    * ranges measured ~20% slower) */
@@ -231,6 +255,7 @@ __global__ void __launch_bounds__(256) k_reduce(const RArgs a) {
 template <class T, int OP, int ORDER, int V, int G, bool MM, int LVL, bool POW2>
 __global__ void __launch_bounds__(256) k_reduce_coop(const RArgs a) {
   typedef Pack<T, V> PK;
+  if constexpr (MM) allow_dependents();
   constexpr int COLS = 32 / G; /* packs per warp per iteration */
   const int lane = threadIdx.x & 31;
   const int g = lane & (G - 1), c = lane / G;
@@ -534,8 +559,18 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
     count_launch();
   }
   if constexpr (MM) {
-    k_minmax_fix<T, OP><<<2 * grid_sms(), 256, 0, s>>>(base, base.fix_list, base.fix_count,
-                                                         base.fix_cap);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * grid_sms());
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, k_minmax_fix<T, OP>, base,
+                             (const unsigned long long *)base.fix_list, base.fix_count,
+                             base.fix_done, base.fix_cap);
     count_launch();
   }
 }
@@ -557,7 +592,7 @@ int run(const RArgs &base, bool aligned, cudaStream_t s) {
 template <class T, int OP>
 int run_float(const RArgs &a, bool aligned, cudaStream_t s) {
   if constexpr (OP == B200SHM_MIN || OP == B200SHM_MAX) {
-    B200_CK(cudaMemsetAsync(a.fix_count, 0, sizeof(unsigned long long), s));
+    /* the deferred count is zero here: the previous replay cleared it */
     return run<T, OP, ORD_CHAIN, true>(a, aligned, s);
   } else {
     switch (a.algo) {
@@ -645,6 +680,9 @@ static RArgs reduce_args(const char *src, char *dst, uint64_t sstep, uint64_t ds
   a.p2s = p2s;
   a.logp2s = logp;
   a.algo = algo;
+  a.fix_list = a.fix_count = a.fix_done = nullptr;
+  a.fix_cap = 0;
+  a.status = nullptr;
   return a;
 }
 
@@ -667,7 +705,8 @@ int reduce_launch(int op, int dtype, int algo, int pe_start, int pe_stride, int 
   RArgs a = reduce_args(m.first + src_off, m.first + dest_off, m.step, m.step, pe_size, nelems,
                         algo);
   a.fix_list = st().fix_list;
-  a.fix_count = st().fix_count;
+  a.fix_count = st().call_fix;
+  a.fix_done = st().call_fix + 1;
   a.fix_cap = st().fix_cap;
   a.status = st().d_status;
   const bool aligned = ((src_off | dest_off | m.step) & 15u) == 0;
@@ -688,7 +727,8 @@ int reduce_range_launch(int op, int dtype, int algo, int pe_start, int pe_stride
   a.g_off = e0;
   a.g_n = nelems;
   a.fix_list = st().fix_list;
-  a.fix_count = st().fix_count;
+  a.fix_count = st().call_fix;
+  a.fix_done = st().call_fix + 1;
   a.fix_cap = st().fix_cap;
   a.status = st().d_status;
   const bool aligned = (((src_off + e0 * es) | (dest_off + e0 * es) | m.step) & 15u) == 0;
@@ -858,7 +898,8 @@ namespace b200 {
 /* at most this many elements per member for a float MIN/MAX reduction,
  * since in the worst case every element is deferred */
 constexpr uint64_t kNoAllocMaxDeferred = 1ull << 18;
-/* [0] deferred count, [1] status bits, [32 ..] deferred element indices:
+/* [0] deferred count, [1] status bits, [2] the replay's exit counter,
+ * [32 ..] deferred element indices:
  * 2 MiB + 256 bytes */
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[32 + kNoAllocMaxDeferred];
 
@@ -943,11 +984,12 @@ extern "C" int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, voi
                         nelems, algo);
   a.fix_count = scratch;
   a.status = (int *)(scratch + 1);
+  a.fix_done = scratch + 2;
   a.fix_list = scratch + 32;
   a.fix_cap = kNoAllocMaxDeferred;
-  /* the scratch keeps the previous call's contents: clear the counter and
-   * the status word first */
-  B200_CK(cudaMemsetAsync(scratch, 0, 2 * sizeof(unsigned long long), s));
+  /* the scratch keeps the previous call's contents: clear the counter, the
+   * status word and the replay's exit counter first */
+  B200_CK(cudaMemsetAsync(scratch, 0, 3 * sizeof(unsigned long long), s));
   const bool aligned = (((uintptr_t)dest | (uintptr_t)source | dest_stride | source_stride) & 15u) == 0;
   if ((rc = reduce_dispatch(op, dtype, a, aligned, s))) return rc;
   cudaError_t e = cudaGetLastError();

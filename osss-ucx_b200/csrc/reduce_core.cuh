@@ -205,6 +205,7 @@ struct RArgs {
   uint64_t g_n;     /* elements of the whole reduction         */
   int P, p2s, logp2s, algo;
   unsigned long long *fix_list, *fix_count; /* deferred elements */
+  unsigned long long *fix_done;  /* k_minmax_fix's exit counter (clears fix_count) */
   unsigned long long fix_cap;
   int *status;
 };

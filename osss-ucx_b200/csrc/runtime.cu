@@ -158,6 +158,8 @@ int b200shm_init(int npes, uint64_t heap_bytes_per_pe, int flags) {
   s.fix_cap = 1ull << 22;
   if (e == cudaSuccess) e = cudaMalloc((void **)&s.fix_list, s.fix_cap * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc((void **)&s.fix_count, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&s.call_fix, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(s.call_fix, 0, 2 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaFree(s.base);
@@ -165,6 +167,7 @@ int b200shm_init(int npes, uint64_t heap_bytes_per_pe, int flags) {
     cudaFreeHost(s.h_status);
     cudaFree(s.fix_list);
     cudaFree(s.fix_count);
+    cudaFree(s.call_fix);
     s = State();
     return cuda_fail(e, "b200shm_init");
   }
@@ -178,6 +181,7 @@ int b200shm_init(int npes, uint64_t heap_bytes_per_pe, int flags) {
     cudaFreeHost(s.h_status);
     cudaFree(s.fix_list);
     cudaFree(s.fix_count);
+    cudaFree(s.call_fix);
     s = State();
     return hrc;
   }
@@ -195,6 +199,7 @@ int b200shm_finalize(void) {
   cudaFreeHost(s.h_status);
   cudaFree(s.fix_list);
   cudaFree(s.fix_count);
+  cudaFree(s.call_fix);
   heap_teardown();
   span_teardown();
   s = State();

@@ -205,11 +205,12 @@ __global__ void k_barrier(const BArgs a) {
 }
 
 /* a team of up to 256 members as one CTA, flags in its shared memory
- * (zeroed before any context pokes one; the contexts that do not take
- * part leave only after that) */
+ * (the P members' lines zeroed before any context pokes one -- no member
+ * touches another line; the contexts that do not take part leave only
+ * after that) */
 __global__ void __launch_bounds__(256) k_barrier_cta(const BArgs a) {
   __shared__ unsigned long long sfl[256 * kCtaRounds];
-  for (int i = threadIdx.x; i < 256 * kCtaRounds; i += blockDim.x) sfl[i] = 0;
+  for (int i = threadIdx.x; i < a.P * kCtaRounds; i += blockDim.x) sfl[i] = 0;
   __syncthreads();
   const int me = threadIdx.x;
   if (me >= a.P || me == a.absent) return;
