@@ -37,9 +37,19 @@ __device__ __forceinline__ void st16(char *p, uint4 u) {
                : "memory");
 }
 
+/* streaming store (evict-first in L2): for data this kernel does not read
+ * again, such as fcollect's P copies of each source vector */
+__device__ __forceinline__ void st16cs(char *p, uint4 u) {
+  asm volatile("st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y), "r"(u.z),
+               "r"(u.w)
+               : "memory");
+}
+
 /* fcollect: member j's dest[k*nbytes + b] = member k's src[b].
  * blockIdx.y = source member k; each thread reads one vector of k's
- * source once and writes it into every member's dest. */
+ * source once and writes it into every member's dest (streaming stores:
+ * 5.99 against 5.92 TB/s with write-back stores, and 5.93 with each CTA
+ * starting at its own member, on 128 members x 32 KiB). */
 template <bool VEC>
 __global__ void __launch_bounds__(256) k_fcollect(const char *src0, char *dst0, uint64_t step,
                                                   int P, uint64_t nbytes) {
@@ -51,7 +61,7 @@ __global__ void __launch_bounds__(256) k_fcollect(const char *src0, char *dst0, 
        v += (uint64_t)gridDim.x * blockDim.x) {
     if constexpr (VEC) {
       const uint4 u = ld16(src + v * 16);
-      for (int j = 0; j < P; j++) st16(dst + (uint64_t)j * step + v * 16, u);
+      for (int j = 0; j < P; j++) st16cs(dst + (uint64_t)j * step + v * 16, u);
     } else {
       const char c = src[v];
       for (int j = 0; j < P; j++) dst[(uint64_t)j * step + v] = c;

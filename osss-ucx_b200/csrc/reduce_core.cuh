@@ -117,6 +117,18 @@ struct alignas(V * sizeof(T) >= 16 ? 16 : alignof(T)) Pack {
   T x[V];
 };
 
+/* Cache policy of the pack accesses: every source and dest byte of a
+ * reduction is touched once, so loads and stores are streaming (.cs:
+ * evict-first in L1 and L2), which keeps fewer of a launch's dirty dest
+ * lines in L2 for the next launch to write back.  On the 64-member x 2^20
+ * headline step (six back-to-back reductions) streaming stores took the
+ * step from 5928 to 6028 GB/s and streaming loads added ~0.1 %. */
+#ifndef B200_LD_OP
+#define B200_LD_OP "ld.global.cs.nc"
+#endif
+#ifndef B200_ST_OP
+#define B200_ST_OP "st.global.cs"
+#endif
 /* 16-byte packs move with one vector access whose registers have the
  * element's own class (f64 pairs, u64, f32, u32), so no moves are needed
  * between the load and the arithmetic. */
@@ -124,22 +136,22 @@ template <class T, int V>
 __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
   Pack<T, V> r;
   if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
-    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];"
+    asm(B200_LD_OP ".v2.f64 {%0,%1}, [%2];"
         : "=d"(r.x[0]), "=d"(r.x[1])
         : "l"(p));
   } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_integral<T>::value &&
                        sizeof(T) == 8) {
     unsigned long long a, b;
-    asm("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+    asm(B200_LD_OP ".v2.u64 {%0,%1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
     r.x[0] = (T)a;
     r.x[1] = (T)b;
   } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, float>::value) {
-    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+    asm(B200_LD_OP ".v4.f32 {%0,%1,%2,%3}, [%4];"
         : "=f"(r.x[0]), "=f"(r.x[1]), "=f"(r.x[2]), "=f"(r.x[3])
         : "l"(p));
   } else if constexpr (sizeof(Pack<T, V>) == 16) {
     uint4 u;
-    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+    asm(B200_LD_OP ".v4.u32 {%0,%1,%2,%3}, [%4];"
         : "=r"(u.x), "=r"(u.y), "=r"(u.z), "=r"(u.w)
         : "l"(p));
     memcpy(&r, &u, 16);
@@ -151,21 +163,21 @@ __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
 template <class T, int V>
 __device__ __forceinline__ void st_pack(char *p, const Pack<T, V> &v) {
   if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
-    asm volatile("st.global.v2.f64 [%0], {%1,%2};" ::"l"(p), "d"(v.x[0]), "d"(v.x[1])
+    asm volatile(B200_ST_OP ".v2.f64 [%0], {%1,%2};" ::"l"(p), "d"(v.x[0]), "d"(v.x[1])
                  : "memory");
   } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_integral<T>::value &&
                        sizeof(T) == 8) {
-    asm volatile("st.global.v2.u64 [%0], {%1,%2};" ::"l"(p),
+    asm volatile(B200_ST_OP ".v2.u64 [%0], {%1,%2};" ::"l"(p),
                  "l"((unsigned long long)v.x[0]), "l"((unsigned long long)v.x[1])
                  : "memory");
   } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, float>::value) {
-    asm volatile("st.global.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(v.x[0]), "f"(v.x[1]),
+    asm volatile(B200_ST_OP ".v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(v.x[0]), "f"(v.x[1]),
                  "f"(v.x[2]), "f"(v.x[3])
                  : "memory");
   } else if constexpr (sizeof(Pack<T, V>) == 16) {
     uint4 u;
     memcpy(&u, &v, 16);
-    asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y),
+    asm volatile(B200_ST_OP ".v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y),
                  "r"(u.z), "r"(u.w)
                  : "memory");
   } else {
