@@ -71,6 +71,7 @@ struct BDesc {
 struct BPlan {
   const BDesc *d;
   const uint32_t *prefix; /* ndesc + 1 tile prefix sums */
+  const uint2 *tile_map;  /* per tile of the plan: (descriptor, tile within it) */
   uint32_t ndesc, total;
   unsigned long long *fix_list, *fix_count;
   unsigned long long fix_cap;
@@ -416,20 +417,17 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_group(const BPlan p,
   /* 16-byte packs: 4 words per level per thread (chains keep no stack) */
   __shared__ uint32_t s_stk[ORDER == ORD_CHAIN ? 1 : kBatchStackLevels * 4 * kBatchThreads];
   const uint32_t base = p.prefix[d0], total = p.prefix[d0 + nd] - base;
+  /* A tile's descriptor comes from the plan's tile map in one load, not
+   * from a binary search over the group's descriptors. */
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
     __syncthreads();
     const unsigned t = s_tile;
     __syncthreads();
     if (t >= total) return;
-    uint32_t lo = d0, hi = d0 + nd; /* prefix[lo] <= base + t < prefix[lo + 1] */
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (p.prefix[mid] <= base + t) lo = mid;
-      else hi = mid;
-    }
-    const BDesc d = p.d[lo];
-    run_desc_tile<T, OP, ORDER, MM, U>(d, lo, base + t - p.prefix[lo], p, s_stk);
+    const uint2 m = p.tile_map[base + t];
+    const BDesc d = p.d[m.x];
+    run_desc_tile<T, OP, ORDER, MM, U>(d, m.x, m.y, p, s_stk);
   }
 }
 
@@ -582,6 +580,7 @@ struct Batch {
   std::vector<b200shm_reduce_desc> fallback; /* run as separate launches */
   BDesc *dd = nullptr;
   uint32_t *dp = nullptr;
+  uint2 *dmap = nullptr; /* tile map (BPlan::tile_map) */
   unsigned *dcount = nullptr;
   bool any_mm = false;
   cudaGraph_t graph = nullptr;
@@ -607,9 +606,11 @@ void release(Batch &b) {
   b.ev.clear();
   if (b.dd) cudaFreeAsync(b.dd, st().stream);
   if (b.dp) cudaFreeAsync(b.dp, st().stream);
+  if (b.dmap) cudaFreeAsync(b.dmap, st().stream);
   if (b.dcount) cudaFreeAsync(b.dcount, st().stream);
   b.dd = nullptr;
   b.dp = nullptr;
+  b.dmap = nullptr;
   b.dcount = nullptr;
 }
 
@@ -633,6 +634,7 @@ BPlan plan_of(const Batch &b) {
   BPlan p;
   p.d = b.dd;
   p.prefix = b.dp;
+  p.tile_map = b.dmap;
   p.ndesc = (uint32_t)b.hd.size();
   p.total = b.hp.empty() ? 0 : b.hp.back();
   p.fix_list = st().fix_list;
@@ -759,6 +761,13 @@ int upload(Batch &b) {
   cudaStream_t ls = st().stream;
   B200_CK(cudaMallocAsync((void **)&b.dd, nd * sizeof(BDesc), ls));
   B200_CK(cudaMallocAsync((void **)&b.dp, (nd + 1) * sizeof(uint32_t), ls));
+  const uint32_t ntiles = b.hp[nd];
+  std::vector<uint2> map(ntiles ? ntiles : 1);
+  for (size_t i = 0; i < nd; i++)
+    for (uint32_t t = b.hp[i]; t < b.hp[i + 1]; t++) map[t] = make_uint2((unsigned)i, t - b.hp[i]);
+  B200_CK(cudaMallocAsync((void **)&b.dmap, map.size() * sizeof(uint2), ls));
+  B200_CK(cudaMemcpyAsync(b.dmap, map.data(), map.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                          ls));
   B200_CK(cudaMallocAsync((void **)&b.dcount, b.groups.size() * sizeof(unsigned), ls));
   B200_CK(cudaMemcpyAsync(b.dd, b.hd.data(), nd * sizeof(BDesc), cudaMemcpyHostToDevice, ls));
   B200_CK(cudaMemcpyAsync(b.dp, b.hp.data(), (nd + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
