@@ -56,8 +56,16 @@ __device__ __forceinline__ uint4 ld16(const char *p) {
                : "l"(p));
   return u;
 }
+/* Stores are streaming (evict-first): every byte written here is written
+ * once and not read again by the kernel.  The fcollect span kernel (one
+ * read, L writes of each byte) ran 5.99 TB/s with them against 5.21 with
+ * write-back stores on 8 ranks x 8 members x 256 KiB; alltoall moved the
+ * same either way. */
+#ifndef B200_SPAN_ST
+#define B200_SPAN_ST "st.global.cs"
+#endif
 __device__ __forceinline__ void st16(char *p, uint4 u) {
-  asm volatile("st.global.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y), "r"(u.z),
+  asm volatile(B200_SPAN_ST ".v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(u.x), "r"(u.y), "r"(u.z),
                "r"(u.w)
                : "memory");
 }
