@@ -498,7 +498,7 @@ void launch_coop(int G, int lvl, bool pow2, uint64_t lanes, cudaStream_t s, cons
 }
 
 template <class T, int OP, int ORDER, bool MM, int LV>
-void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
+int run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
   constexpr int V = sizeof(T) >= 16 ? 1 : (int)(16 / sizeof(T));
   constexpr int U = ORDER == ORD_CHAIN ? 8 : 4;
   static int occ_pack = -1, occ_tail = -1;
@@ -568,25 +568,23 @@ void run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    (void)cudaLaunchKernelEx(&cfg, k_minmax_fix<T, OP>, base,
-                             (const unsigned long long *)base.fix_list, base.fix_count,
-                             base.fix_done, base.fix_cap);
+    B200_CK(cudaLaunchKernelEx(&cfg, k_minmax_fix<T, OP>, base,
+                               (const unsigned long long *)base.fix_list, base.fix_count,
+                               base.fix_done, base.fix_cap));
     count_launch();
   }
+  return B200SHM_OK;
 }
 
 template <class T, int OP, int ORDER, bool MM>
 int run(const RArgs &base, bool aligned, cudaStream_t s) {
   if constexpr (ORDER == ORD_CHAIN) {
-    run_lv<T, OP, ORDER, MM, 1>(base, aligned, s);
+    return run_lv<T, OP, ORDER, MM, 1>(base, aligned, s);
   } else {
     const int leaves = ORDER == ORD_BUTTERFLY ? base.p2s : base.P;
-    if (leaves < (1 << 8))
-      run_lv<T, OP, ORDER, MM, 8>(base, aligned, s);
-    else
-      run_lv<T, OP, ORDER, MM, kMaxLevels>(base, aligned, s);
+    if (leaves < (1 << 8)) return run_lv<T, OP, ORDER, MM, 8>(base, aligned, s);
+    return run_lv<T, OP, ORDER, MM, kMaxLevels>(base, aligned, s);
   }
-  return B200SHM_OK;
 }
 
 template <class T, int OP>
