@@ -123,6 +123,39 @@ def test_order_dependent_minmax_is_exact(B, heap, rs, algo, dt, op):
         assert got.tobytes() == rs.reduce(algo, op, x).tobytes(), (algo, dt, op, P, N, in_place)
 
 
+@pytest.mark.parametrize("ordered", [False, True])
+@pytest.mark.parametrize("dt", ["float32", "float64"])
+def test_deferred_list_starts_empty_every_call(B, heap, rs, dt, ordered):
+    """The replay kernel of a float MIN/MAX call clears the deferred count
+    for the next call (no memset precedes a call).  A call that defers
+    nearly every one of 20000 elements is followed by a 100-element call on
+    other buffers: a stale count would replay indices far past its rows and
+    overwrite the guard bytes after them.  Then a small special-value call.
+    `ordered`: the three calls back to back on the engine stream."""
+    P = 16
+    x1 = special(oracle.NP[dt], P, 20000, 7)
+    x2 = gen.normal(oracle.NP[dt], P, 100, 8)
+    x3 = special(oracle.NP[dt], P, 37, 9)
+    guard = 4096
+    bufs = []
+    for x in (x1, x2, x3):
+        nb = x[0].nbytes
+        src, dst = heap(nb), heap(nb + guard)
+        B.put_rows(src, x, team=(0, 1, P))
+        B.memset(dst, 0xA5, nb + guard, team=(0, 1, P))
+        bufs.append((src, dst, nb))
+    stream = B.stream() if ordered else None
+    for (src, dst, nb), x in zip(bufs, (x1, x2, x3)):
+        B.reduce("max", dt, "rec_dbl", dst, src, x.shape[1], team=(0, 1, P), stream=stream)
+    if ordered:
+        B.quiet()
+    for (src, dst, nb), x in zip(bufs, (x1, x2, x3)):
+        got = B.get_rows(dst, nb + guard, np.uint8, team=(0, 1, P))
+        want = rs.reduce("rec_dbl", "max", x)
+        assert got[:, :nb].tobytes() == want.view(np.uint8).tobytes(), (dt, x.shape)
+        assert (got[:, nb:] == 0xA5).all(), "bytes after the dest rows were written"
+
+
 @pytest.mark.parametrize("dt", ["complex64", "complex128"])
 def test_complex_prod_with_infinities(B, heap, rs, dt):
     rng = np.random.default_rng(5)
