@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) k_minmax_fix(const RArgs a,
                                                     unsigned long long *count,
                                                     unsigned long long *done,
                                                     unsigned long long cap) {
-  __shared__ T vals[kFixMaxMembers];
+  __shared__ T vals[fix_max_members<T>()];
   __shared__ T common;
   asm volatile("griddepcontrol.wait;" ::: "memory");
   const unsigned long long cnt = *(volatile unsigned long long *)count;
@@ -640,9 +640,6 @@ static int reduce_check(int op, int dtype, int algo, int pe_size) {
   const bool is_cpx = dtype == B200SHM_C32 || dtype == B200SHM_C64;
   if ((op <= B200SHM_XOR && !is_int) || ((op == B200SHM_MIN || op == B200SHM_MAX) && is_cpx))
     return fail(B200SHM_ERR_UNSUPPORTED, "reduce: op %d is not defined on dtype %d", op, dtype);
-  if (dtype == B200SHM_F80)
-    return fail(B200SHM_ERR_UNSUPPORTED,
-                "reduce: long double (x87 80-bit) arithmetic is not available on the GPU");
   if (pe_size < 1) return fail(B200SHM_ERR_ARG, "reduce: team size %d < 1", pe_size);
   int p2s = 1;
   while (p2s * 2 <= pe_size) p2s *= 2;
@@ -651,6 +648,10 @@ static int reduce_check(int op, int dtype, int algo, int pe_size) {
   if (tree && leaves > (1 << (kMaxLevels - 1)))
     return fail(B200SHM_ERR_UNSUPPORTED, "reduce: float combine trees are limited to %d members",
                 1 << (kMaxLevels - 1));
+  if (dtype == B200SHM_F80 && (op == B200SHM_MIN || op == B200SHM_MAX) &&
+      pe_size > kFixMaxMembersF80)
+    return fail(B200SHM_ERR_UNSUPPORTED, "reduce: long double MIN/MAX is limited to %d members",
+                kFixMaxMembersF80);
   if (!is_int && (op == B200SHM_MIN || op == B200SHM_MAX) && pe_size > kFixMaxMembers)
     return fail(B200SHM_ERR_UNSUPPORTED, "reduce: float MIN/MAX is limited to %d members",
                 kFixMaxMembers);
@@ -756,6 +757,13 @@ static int reduce_dispatch(int op, int dtype, const RArgs &a, bool aligned, cuda
     case B200SHM_MAX: return run_float<double, B200SHM_MAX>(a, aligned, s);
     case B200SHM_SUM: return run_float<double, B200SHM_SUM>(a, aligned, s);
     default: return run_float<double, B200SHM_PROD>(a, aligned, s);
+    }
+  case B200SHM_F80:
+    switch (op) {
+    case B200SHM_MIN: return run_float<f80, B200SHM_MIN>(a, aligned, s);
+    case B200SHM_MAX: return run_float<f80, B200SHM_MAX>(a, aligned, s);
+    case B200SHM_SUM: return run_float<f80, B200SHM_SUM>(a, aligned, s);
+    default: return run_float<f80, B200SHM_PROD>(a, aligned, s);
     }
   case B200SHM_C32:
     return op == B200SHM_SUM ? run_cplx<cf32, B200SHM_SUM>(a, aligned, s)
@@ -969,7 +977,8 @@ extern "C" int b200shm_reduce_noalloc(int op, int dtype, int algo, int npes, voi
     }
   }
   const bool minmax_float = (op == B200SHM_MIN || op == B200SHM_MAX) &&
-                            (dtype == B200SHM_F32 || dtype == B200SHM_F64);
+                            (dtype == B200SHM_F32 || dtype == B200SHM_F64 ||
+                             dtype == B200SHM_F80);
   if (minmax_float && nelems > kNoAllocMaxDeferred)
     return fail(B200SHM_ERR_UNSUPPORTED,
                 "reduce_noalloc: float MIN/MAX is limited to %llu elements per member (the "

@@ -11,6 +11,7 @@
 
 #include <type_traits>
 
+#include "f80.cuh"
 #include "internal.cuh"
 
 namespace b200 {
@@ -97,6 +98,12 @@ template <int OP, class T>
 __device__ __forceinline__ T apply(T a, T b) {
   if constexpr (std::is_same<T, float>::value || std::is_same<T, double>::value) {
     return op_flt<OP>(a, b);
+  } else if constexpr (std::is_same<T, f80>::value) {
+    /* x87 long double, as reduce.c:730-736 evaluate it on the host */
+    if constexpr (OP == B200SHM_MIN) return f80_lt(a, b) ? a : b;
+    else if constexpr (OP == B200SHM_MAX) return f80_gt(a, b) ? a : b;
+    else if constexpr (OP == B200SHM_SUM) return f80_add(a, b);
+    else return f80_mul(a, b);
   } else if constexpr (std::is_same<T, cf32>::value || std::is_same<T, cf64>::value) {
     T r;
     if constexpr (OP == B200SHM_SUM) {
@@ -203,6 +210,14 @@ __device__ __forceinline__ unsigned fclass(double f) {
   return ((u & 0x7fffffffffffffffull) > 0x7ff0000000000000ull ? 1u : 0u) |
          (u == 0ull ? 2u : 0u) | (u == 0x8000000000000000ull ? 4u : 0u);
 }
+/* long double: bit 0 also for the operands whose comparisons are
+ * unordered (unsupported encodings) and for pseudo-denormals, which compare
+ * equal to the normal of the same value with other bits */
+__device__ __forceinline__ unsigned fclass(const f80 &f) {
+  if (f80_is_nan(f) || f80_is_unsupported(f) || f80_is_pseudo_denormal(f)) return 1u;
+  if (f80_is_zero(f)) return (f.se & 0x8000) ? 4u : 2u;
+  return 0u;
+}
 __device__ __forceinline__ bool ambiguous(unsigned f) { return (f & 1u) || (f & 6u) == 6u; }
 
 struct RArgs {
@@ -303,6 +318,13 @@ __device__ __forceinline__ int rev_bits(int x, int n) {
 }
 
 constexpr int kFixMaxMembers = 4096;
+/* members of a long double MIN/MAX team (the replay stages the P inputs of
+ * 16 bytes each in shared memory) */
+constexpr int kFixMaxMembersF80 = 2048;
+template <class T>
+constexpr int fix_max_members() {
+  return sizeof(T) > 8 ? kFixMaxMembersF80 : kFixMaxMembers;
+}
 
 template <class T, int V>
 __device__ __forceinline__ Pack<T, V> shfl_xor_pack(const Pack<T, V> &v, int m) {

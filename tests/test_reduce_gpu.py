@@ -211,7 +211,7 @@ def test_reduce_rejects_bad_arguments(B, heap):
     with pytest.raises(B.B200Error):
         B.reduce("xor", "float32", "rec_dbl", src, src, 16, team=(0, 1, 4))
     with pytest.raises(B.B200Error):
-        B.reduce("sum", "float80", "rec_dbl", src, src, 16, team=(0, 1, 4))
+        B.reduce("xor", "float80", "rec_dbl", src, src, 16, team=(0, 1, 4))
     with pytest.raises(B.B200Error):
         B.reduce("sum", "float32", "rec_dbl", src + 8, src, 16, team=(0, 1, 4))  # partial overlap
     with pytest.raises(B.B200Error):
