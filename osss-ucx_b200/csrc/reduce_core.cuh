@@ -136,13 +136,66 @@ struct alignas(V * sizeof(T) >= 16 ? 16 : alignof(T)) Pack {
 #ifndef B200_ST_OP
 #define B200_ST_OP "st.global.cs"
 #endif
+/* One 16-byte element (complex double, long double) at any alignment: one
+ * 16-byte access where the address allows it, else 8-, 4- or 1-byte
+ * pieces.  A complex double array needs only 8-byte alignment, and the
+ * C ABI takes byte offsets, so a single element may sit anywhere; the
+ * branch is uniform across a warp whenever the member rows share their
+ * alignment. */
+__device__ __forceinline__ void ld16_any(const char *p, uint32_t w[4]) {
+  const uintptr_t a = (uintptr_t)p;
+  if ((a & 15) == 0) {
+    asm(B200_LD_OP ".v4.u32 {%0,%1,%2,%3}, [%4];"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+        : "l"(p));
+  } else if ((a & 7) == 0) {
+    asm(B200_LD_OP ".v2.u32 {%0,%1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "l"(p));
+    asm(B200_LD_OP ".v2.u32 {%0,%1}, [%2];" : "=r"(w[2]), "=r"(w[3]) : "l"(p + 8));
+  } else if ((a & 3) == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) asm(B200_LD_OP ".u32 %0, [%1];" : "=r"(w[i]) : "l"(p + 4 * i));
+  } else {
+    unsigned char b[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) b[i] = (unsigned char)p[i];
+    memcpy(w, b, 16);
+  }
+}
+__device__ __forceinline__ void st16_any(char *p, const uint32_t w[4]) {
+  const uintptr_t a = (uintptr_t)p;
+  if ((a & 15) == 0) {
+    asm volatile(B200_ST_OP ".v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(w[0]), "r"(w[1]),
+                 "r"(w[2]), "r"(w[3])
+                 : "memory");
+  } else if ((a & 7) == 0) {
+    asm volatile(B200_ST_OP ".v2.u32 [%0], {%1,%2};" ::"l"(p), "r"(w[0]), "r"(w[1]) : "memory");
+    asm volatile(B200_ST_OP ".v2.u32 [%0], {%1,%2};" ::"l"(p + 8), "r"(w[2]), "r"(w[3])
+                 : "memory");
+  } else if ((a & 3) == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      asm volatile(B200_ST_OP ".u32 [%0], %1;" ::"l"(p + 4 * i), "r"(w[i]) : "memory");
+  } else {
+    unsigned char b[16];
+    memcpy(b, w, 16);
+#pragma unroll
+    for (int i = 0; i < 16; i++) p[i] = (char)b[i];
+  }
+}
+
 /* 16-byte packs move with one vector access whose registers have the
  * element's own class (f64 pairs, u64, f32, u32), so no moves are needed
- * between the load and the arithmetic. */
+ * between the load and the arithmetic.  Packs of several elements are
+ * used only on 16-byte-aligned rows; a pack of one 16-byte element may be
+ * at any alignment. */
 template <class T, int V>
 __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
   Pack<T, V> r;
-  if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
+  if constexpr (sizeof(Pack<T, V>) == 16 && V == 1) {
+    uint32_t w[4];
+    ld16_any(p, w);
+    memcpy(&r, w, 16);
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
     asm(B200_LD_OP ".v2.f64 {%0,%1}, [%2];"
         : "=d"(r.x[0]), "=d"(r.x[1])
         : "l"(p));
@@ -169,7 +222,11 @@ __device__ __forceinline__ Pack<T, V> ld_pack(const char *p) {
 }
 template <class T, int V>
 __device__ __forceinline__ void st_pack(char *p, const Pack<T, V> &v) {
-  if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
+  if constexpr (sizeof(Pack<T, V>) == 16 && V == 1) {
+    uint32_t w[4];
+    memcpy(w, &v, 16);
+    st16_any(p, w);
+  } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_same<T, double>::value) {
     asm volatile(B200_ST_OP ".v2.f64 [%0], {%1,%2};" ::"l"(p), "d"(v.x[0]), "d"(v.x[1])
                  : "memory");
   } else if constexpr (sizeof(Pack<T, V>) == 16 && std::is_integral<T>::value &&

@@ -11,7 +11,8 @@ from test_reduce_gpu import nan_equal_bytes
 pytestmark = pytest.mark.gpu
 
 NP_T = {"int32": np.int32, "int64": np.int64, "uint32": np.uint32, "uint64": np.uint64,
-        "float32": np.float32, "float64": np.float64, "int16": np.int16, "complex64": np.complex64}
+        "float32": np.float32, "float64": np.float64, "int16": np.int16, "complex64": np.complex64,
+        "float80": np.longdouble}
 
 
 def make_batch(B, heap, rng, n, npes, sizes=(1, 2, 3, 5, 8, 13, 16, 31, 64),
@@ -24,7 +25,7 @@ def make_batch(B, heap, rng, n, npes, sizes=(1, 2, 3, 5, 8, 13, 16, 31, 64),
             stride = 1
         start = int(rng.integers(0, npes - (size - 1) * stride))
         dt = str(rng.choice(["int32", "int64", "uint32", "uint64", "float32", "float64",
-                             "int16", "complex64"]))
+                             "int16", "complex64", "float80"]))
         if dt.startswith(("int", "uint")):
             op = str(rng.choice(oracle.OPS))
         elif dt == "complex64":
@@ -67,7 +68,7 @@ def per_call(B, items, inputs):
 def check_oracle(rs, items, inputs, got, every=7):
     for k in range(0, len(items), every):
         it, x = items[k], inputs[k]
-        if it["dtype"] == "complex64" or (it["op"] in ("sum", "prod") and
+        if it["dtype"] in ("complex64", "float80") or (it["op"] in ("sum", "prod") and
                                           it["dtype"].startswith("float") and
                                           it["algo"] == "binomial"):
             continue  # the oracle's binomial float order is arrival-dependent
@@ -92,7 +93,8 @@ def test_batch_matches_per_call_and_oracle(B, heap, rs, flags):
     b.close()
     assert all(d.algo >= 0 for d in descs)  # AUTO rewritten to a concrete order
     assert any(d.lanes > 1 for d in descs)
-    assert all(d.lanes == 0 for d, it in zip(descs, items) if it["dtype"] in ("int16", "complex64"))
+    assert all(d.lanes == 0 for d, it in zip(descs, items)
+               if it["dtype"] in ("int16", "complex64", "float80"))
     check_oracle(rs, items, inputs, got)
 
 

@@ -156,6 +156,26 @@ def test_deferred_list_starts_empty_every_call(B, heap, rs, dt, ordered):
         assert (got[:, nb:] == 0xA5).all(), "bytes after the dest rows were written"
 
 
+@pytest.mark.parametrize("mis", [8, 4, 1])
+def test_sixteen_byte_elements_at_any_alignment(B, heap, rs, mis):
+    """complex double (8-byte aligned in C) and long double rows at byte
+    offsets that are not multiples of 16: each element moves in 8-, 4- or
+    1-byte pieces there, with the same result bits."""
+    for algo in ("rec_dbl", "linear"):
+        for dt, op in (("complex128", "sum"), ("complex128", "prod"), ("float80", "sum"),
+                       ("float80", "max")):
+            x = gen.random_values(oracle.NP[dt], 6, 37, 17 + mis)
+            if op == "prod":
+                x = (1.0 + 0.01 * x).astype(x.dtype)
+            got = gpu_reduce(B, heap, algo, op, x, misalign=mis)
+            want = rs.reduce(algo, op, x)
+            if dt == "float80":
+                vb = lambda a: np.ascontiguousarray(a).view(np.uint8).reshape(a.shape + (16,))[..., :10]
+                assert vb(got).tobytes() == vb(want).tobytes(), (algo, dt, op, mis)
+            else:
+                assert nan_equal_bytes(got, want), (algo, dt, op, mis)
+
+
 @pytest.mark.parametrize("dt", ["complex64", "complex128"])
 def test_complex_prod_with_infinities(B, heap, rs, dt):
     rng = np.random.default_rng(5)

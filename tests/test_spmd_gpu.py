@@ -294,3 +294,44 @@ def test_spmd_generics_program(tmp_path):
                                        SHMEM_B200_WAIT_TIMEOUT="60"),
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_spmd_longdouble_reductions(tmp_path, rs):
+    """shmem_longdouble_sum_reduce / _prod_reduce over SHMEM_TEAM_WORLD and
+    shmem_longdouble_max_to_all (NaN payloads, signed zeros, infinities
+    among the inputs) from an 8-PE C program, against the oracle on the
+    10 value bytes of every element (tests/c/spmd_longdouble.c)."""
+    import __graft_entry__
+    __graft_entry__.build_library()
+    exe = str(tmp_path / "spmd_longdouble")
+    subprocess.run(["gcc", "-std=gnu11", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "spmd_longdouble.c"), "-L" + LIB,
+                    "-lshmem_b200", "-Wl,-rpath," + LIB, "-o", exe], check=True)
+    P, N = 8, 300
+    rng = np.random.default_rng(11)
+    s = (1.0 + rng.uniform(-0.25, 0.25, (P, N))).astype(np.longdouble)
+    s *= (1.0 + np.longdouble(2.0) ** -40 * rng.integers(0, 1 << 20, (P, N)))  # full significands
+    m = rng.uniform(-1e6, 1e6, (P, N)).astype(np.longdouble)
+    pick = rng.integers(0, 8, size=(P, N))
+    m[pick == 0] = 0.0
+    m[pick == 1] = -0.0
+    m[pick == 2] = np.nan
+    m[pick == 3] = -np.inf
+    inp, outp = tmp_path / "in.bin", tmp_path / "out.bin"
+    with open(inp, "wb") as f:
+        f.write(np.ascontiguousarray(s).tobytes())
+        f.write(np.ascontiguousarray(m).tobytes())
+    r = subprocess.run([exe, str(inp), str(outp)], env=dict(os.environ, SHMEM_SYMMETRIC_SIZE="8M"),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(outp, dtype=np.uint8)
+    n = P * N * 16
+    got = [raw[i * n:(i + 1) * n].view(np.longdouble).reshape(P, N) for i in range(3)]
+    assert (raw[3 * n:].view(np.int32) == 0).all()
+
+    def vb(a):
+        return np.ascontiguousarray(a).view(np.uint8).reshape(P, N, 16)[..., :10].tobytes()
+    assert vb(got[0]) == vb(rs.reduce("rec_dbl", "sum", s))
+    assert vb(got[1]) == vb(rs.reduce("rec_dbl", "prod", s))
+    assert vb(got[2]) == vb(rs.reduce("rec_dbl", "max", m))
