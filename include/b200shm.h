@@ -119,7 +119,9 @@ int b200shm_memset(int pe_start, int pe_stride, int pe_count, uint64_t off,
  * rabenseifner2} (src/shcoll/src/reduce.c:55-724) behind
  * shcoll_<T>_<op>_reduce_<algo> (reduce.c:1078-1102) and
  * shcoll_<T>_<op>_to_all_<algo> (reduce.c:931-955).  dest_off == src_off
- * (in place) is allowed; other overlaps are rejected. */
+ * (in place) is allowed; other overlaps are rejected.  Long double
+ * (B200SHM_F80, MIN/MAX/SUM/PROD) runs on a software x87 whose bits equal
+ * an x86 host's; its MIN/MAX teams are limited to 2048 members. */
 int b200shm_reduce(int op, int dtype, int algo, int pe_start, int pe_stride,
                    int pe_size, uint64_t dest_off, uint64_t src_off,
                    uint64_t nelems, void *stream);
