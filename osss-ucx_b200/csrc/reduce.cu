@@ -504,7 +504,12 @@ int run_lv(const RArgs &base, bool aligned, cudaStream_t s) {
   static int occ_pack = -1, occ_tail = -1;
   RArgs a = base;
   uint64_t done = 0;
-  if (aligned && V > 1 && done < base.N) {
+  /* packs of several elements need 16-byte-aligned rows; a pack of one
+   * 16-byte element (complex double, long double) moves at any alignment,
+   * and its trees split over lanes too (long double SUM 1.52 -> 2.11 TB/s,
+   * PROD 2.20 -> 3.16 on 64 members x 2^18), while its chains stay one
+   * lane per element (long double MAX split over lanes: 2.56 -> 2.11) */
+  if ((V > 1 ? aligned : ORDER != ORD_CHAIN) && done < base.N) {
     a.e_begin = done;
     a.nvec = (base.N - done) / V;
     if (a.nvec) {
