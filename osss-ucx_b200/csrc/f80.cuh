@@ -99,6 +99,7 @@ B200_F80_FN void f80_unpack(const f80 &a, uint64_t &m, int &e) {
 /* Round the non-zero value M * 2^(e - bias - 125) once to nearest even on
  * the extended grid and encode it. */
 B200_F80_FN f80 f80_round_pack(unsigned sign, int e, f80_u128 M) {
+  if (M == 0) return f80_make((uint16_t)(sign << 15), 0); /* not reached by the callers */
   /* the most significant bit of M to bit 125 */
   int msb = 127;
   while (!((M >> msb) & 1)) msb--;
