@@ -101,8 +101,8 @@ B200_F80_FN void f80_unpack(const f80 &a, uint64_t &m, int &e) {
 B200_F80_FN f80 f80_round_pack(unsigned sign, int e, f80_u128 M) {
   if (M == 0) return f80_make((uint16_t)(sign << 15), 0); /* not reached by the callers */
   /* the most significant bit of M to bit 125 */
-  int msb = 127;
-  while (!((M >> msb) & 1)) msb--;
+  const uint64_t hi = (uint64_t)(M >> 64), lo = (uint64_t)M;
+  const int msb = hi ? 127 - f80_clz64(hi) : 63 - f80_clz64(lo);
   if (msb > 125) {
     const int sh = msb - 125;
     const bool sticky = (M & ((((f80_u128)1) << sh) - 1)) != 0;
