@@ -51,7 +51,10 @@ def build(verbose=False, extra=()):
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB, exist_ok=True)
     heads = _headers()
-    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    # the long double reduce units (software x87 arithmetic in every
+    # instantiation) take far longer than the rest: start them first
+    srcs = sorted((os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")),
+                  key=lambda p: (not os.path.basename(p).startswith("reduce_f80_"), p))
     lib = os.path.join(LIB, CUDA_LIB)
     if not extra and not _stale(lib, srcs + heads + [__file__]):
         build_host(lib)
@@ -63,7 +66,8 @@ def build(verbose=False, extra=()):
         objs.append(o)
         if _stale(o, [s] + heads + [__file__]):
             jobs.append((s, o))
-    with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs) or 1)) as ex:
+    workers = max(8, os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=min(workers, len(jobs) or 1)) as ex:
         for o in ex.map(lambda so: _compile(so[0], so[1], extra), jobs):
             if verbose:
                 print("compiled", o)

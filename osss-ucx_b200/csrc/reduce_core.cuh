@@ -1,7 +1,7 @@
 /*
  * reduce_core.cuh -- the element operators, 16-byte packs and exact-order
- * helpers shared by the per-call reduce kernels (reduce.cu) and the batched
- * reduce kernels (batch.cu).  The combine operators follow
+ * helpers shared by the per-call reduce kernels (reduce_kernels.cuh) and the
+ * batched reduce kernels (batch.cu).  The combine operators follow
  * src/shcoll/src/reduce.c:730-736; the tree-order helpers follow the
  * rec_dbl / Rabenseifner extra-PE fold (reduce.c:206-272, 338-454).
  */
@@ -277,6 +277,10 @@ __device__ __forceinline__ unsigned fclass(const f80 &f) {
 }
 __device__ __forceinline__ bool ambiguous(unsigned f) { return (f & 1u) || (f & 6u) == 6u; }
 
+}  // namespace
+
+/* One reduction's launch arguments (outside the unnamed namespace: the
+ * per-family launch sequences below take it across translation units). */
 struct RArgs {
   const char *src;  /* member 0's source at element 0          */
   char *dst;        /* member 0's dest at element 0            */
@@ -293,6 +297,23 @@ struct RArgs {
   unsigned long long fix_cap;
   int *status;
 };
+
+/* The launch sequence of one validated reduction on stream s, one function
+ * per element-type family, each in its own translation unit
+ * (reduce_<family>.cu) so the families' kernels compile in parallel.
+ * `aligned`: every row starts on a 16-byte boundary. */
+int reduce_dispatch_int(int op, int dtype, const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_f32(int op, const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_f64(int op, const RArgs &a, bool aligned, cudaStream_t s);
+/* long double: one function (and translation unit) per op */
+int reduce_dispatch_f80_min(const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_f80_max(const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_f80_sum(const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_f80_prod(const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_c32(int op, const RArgs &a, bool aligned, cudaStream_t s);
+int reduce_dispatch_c64(int op, const RArgs &a, bool aligned, cudaStream_t s);
+
+namespace {
 
 /* p2s membership, reduce.c:206-214 and 232 */
 __device__ __forceinline__ int p2s_member(int q, int P, int p2s) {
