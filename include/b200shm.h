@@ -254,6 +254,13 @@ int b200shm_ipc_handle(void *handle);
 int b200shm_peer_open(const void *handle, void **peer_base);
 int b200shm_peer_close(void *peer_base);
 
+/* Every address the span calls below take (a partial vector, a rank's
+ * arena base) must lie, with everything the call reads through it, inside
+ * this engine's arena or inside an arena mapped with b200shm_peer_open and
+ * still open (a peer arena having this one's npes and slice size); any
+ * other address is refused with B200SHM_ERR_ARG before anything is
+ * launched, zero-size calls included. */
+
 /* The cross-GPU half of a reduction over a team of G x pe_count members
  * (pe_count on each of G GPUs, G a power of two up to 16), fused with its
  * write-back: element by element, the G ranks' partial vectors -- each the

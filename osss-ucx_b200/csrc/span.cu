@@ -287,6 +287,35 @@ int span_check(int G, int rank, const uint64_t *addrs, int pe_start, int pe_stri
   return check_team(pe_start, pe_stride, L);
 }
 
+/* [a, a + bytes) lies wholly inside this process's arena or inside an open
+ * peer mapping.  A peer's arena has this one's geometry (npes slices of
+ * `slice` bytes): every rank of a spanning team initialises the engine with
+ * the same PE count and heap size.  Checked before any launch, so an
+ * address from nowhere is refused instead of faulting the kernel. */
+bool known_range(uint64_t a, uint64_t bytes) {
+  const uint64_t len = (uint64_t)st().npes * st().slice;
+  auto inside = [&](uint64_t b) { return a >= b && bytes <= len && a - b <= len - bytes; };
+  if (inside((uint64_t)(uintptr_t)st().base)) return true;
+  std::lock_guard<std::mutex> lk(peers().mu);
+  for (const auto &kv : peers().by_handle)
+    if (inside((uint64_t)(uintptr_t)kv.second.base)) return true;
+  return false;
+}
+
+/* Each rank's base, as the span kernels read it: its members' slices
+ * [base + first, base + first + (L-1)*step + slice) are all they touch
+ * there (offsets within a slice are checked separately). */
+int check_bases(const char *what, int G, const uint64_t *bases, uint64_t first, uint64_t step,
+                int L) {
+  const uint64_t span = (uint64_t)(L - 1) * step + st().slice;
+  for (int g = 0; g < G; g++)
+    if (bases[g] > UINT64_MAX - first || !known_range(bases[g] + first, span))
+      return fail(B200SHM_ERR_ARG,
+                  "%s: rank %d's base %#llx is not in this arena or an open peer mapping", what,
+                  g, (unsigned long long)bases[g]);
+  return B200SHM_OK;
+}
+
 }  // namespace
 
 /* at finalize: every peer mapping still open is closed */
@@ -361,6 +390,11 @@ int b200shm_span_combine(int op, int dtype, int G, int rank, const uint64_t *par
   if (dest_off % al) return fail(B200SHM_ERR_ARG, "span_combine: dest misaligned");
   for (int g = 0; g < G; g++)
     if (partials[g] % al) return fail(B200SHM_ERR_ARG, "span_combine: partial %d misaligned", g);
+  for (int g = 0; g < G; g++)
+    if (!known_range(partials[g], nelems * es))
+      return fail(B200SHM_ERR_ARG,
+                  "span_combine: rank %d's partial %#llx is not in this arena or an open peer "
+                  "mapping", g, (unsigned long long)partials[g]);
   if (nelems == 0) return B200SHM_OK;
   /* slot y holds rank (y ^ rank)'s partial: the kernel's static indexing */
   SpanPtrs p{};
@@ -403,11 +437,12 @@ int b200shm_span_fcollect(int G, int rank, const uint64_t *bases, int pe_start, 
     return rc;
   if (overlaps(dest_off, nbytes * M, src_off, nbytes))
     return fail(B200SHM_ERR_ARG, "span_fcollect: dest and source overlap");
+  const uint64_t first = (uint64_t)pe_start * st().slice;
+  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
+  if ((rc = check_bases("span_fcollect", G, bases, first, step, pe_count))) return rc;
   if (nbytes == 0) return B200SHM_OK;
   SpanPtrs p{};
   for (int g = 0; g < G; g++) p.p[g] = (const char *)(uintptr_t)bases[g];
-  const uint64_t first = (uint64_t)pe_start * st().slice;
-  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
   bool vec = ((src_off | dest_off | nbytes | step | first) & 15u) == 0;
   for (int g = 0; g < G; g++) vec = vec && (bases[g] & 15u) == 0;
   const uint64_t n = vec ? nbytes / 16 : nbytes;
@@ -439,11 +474,12 @@ int b200shm_span_alltoall(int G, int rank, const uint64_t *bases, int pe_start, 
     return rc;
   if (overlaps(dest_off, nbytes * M, src_off, nbytes * M))
     return fail(B200SHM_ERR_ARG, "span_alltoall: dest and source overlap");
+  const uint64_t first = (uint64_t)pe_start * st().slice;
+  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
+  if ((rc = check_bases("span_alltoall", G, bases, first, step, pe_count))) return rc;
   if (nbytes == 0) return B200SHM_OK;
   SpanPtrs p{};
   for (int g = 0; g < G; g++) p.p[g] = (const char *)(uintptr_t)bases[g];
-  const uint64_t first = (uint64_t)pe_start * st().slice;
-  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
   bool vec = ((src_off | dest_off | nbytes | step | first) & 15u) == 0;
   for (int g = 0; g < G; g++) vec = vec && (bases[g] & 15u) == 0;
   const uint64_t n = vec ? nbytes / 16 : nbytes;
@@ -479,13 +515,14 @@ int b200shm_span_amo(int amo, int dtype, int G, const uint64_t *bases, int pe_st
     return fail(B200SHM_ERR_UNSUPPORTED, "span_amo: floating types support only swap/set/fetch");
   const bool needs_value = !(amo == B200SHM_AMO_FETCH || amo == B200SHM_AMO_INC ||
                              amo == B200SHM_AMO_FETCH_INC);
+  const uint64_t first = (uint64_t)pe_start * st().slice;
+  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
+  if ((rc = check_bases("span_amo", G, bases, first, step, pe_count))) return rc;
   if (nops == 0) return B200SHM_OK;
   if (!member || !off || (needs_value && !value) || (amo == B200SHM_AMO_CSWAP && !cond))
     return fail(B200SHM_ERR_ARG, "span_amo: missing operand array");
   SpanPtrs p{};
   for (int g = 0; g < G; g++) p.p[g] = (const char *)(uintptr_t)bases[g];
-  const uint64_t first = (uint64_t)pe_start * st().slice;
-  const uint64_t step = (uint64_t)(pe_count > 1 ? pe_stride : 1) * st().slice;
   const int M = G * pe_count;
   const unsigned grid = grid_for(nops, 256, 8);
   cudaStream_t s = pick_stream(stream);

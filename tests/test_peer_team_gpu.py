@@ -226,3 +226,37 @@ def test_peer_team_matches_oracle(world):
                           or op in ("min", "max")
                           or algo in ("rec_dbl", "rabenseifner", "rabenseifner2"))
             assert exact == want_exact, (world, CASES[k])
+
+
+@pytest.mark.gpu
+def test_span_calls_refuse_addresses_outside_any_arena(B, heap):
+    """A rank base or partial that lies in neither this process's arena nor
+    an open peer mapping is refused with ERR_ARG before anything launches.
+    Every call here moves zero bytes, so none of them would launch a kernel
+    even if the check let the address through."""
+    base, sl, npes = B.heap_base(), B.heap_slice(), B.n_pes()
+    end = base + npes * sl
+    dst, src = heap(4096), heap(4096)
+    team = (0, 1, 4)
+    good = [base, base + 4 * sl]
+    # accepted: rank bases whose members' slices lie in this arena
+    B.span_fcollect(2, 0, good, dst, src, 0, team=team)
+    B.span_alltoall(2, 0, good, dst, src, 0, team=team)
+    B.span_amo("fetch_add", "int64", 2, good, 0, 0, 0, team=team)
+    B.span_combine("sum", "float32", 2, 0, [B.ptr(0, src), B.ptr(4, src)], dst, 0, team=team)
+    bad_bases = [
+        [base, end],                 # just past the arena
+        [base, base + (npes - 2) * sl],  # starts inside, its 4 members' slices run past the end
+        [base - 4 * sl, base],       # before the arena
+    ]
+    for bases in bad_bases:
+        for call in (lambda: B.span_fcollect(2, 0, bases, dst, src, 0, team=team),
+                     lambda: B.span_alltoall(2, 0, bases, dst, src, 0, team=team),
+                     lambda: B.span_amo("fetch_add", "int64", 2, bases, 0, 0, 0, team=team)):
+            with pytest.raises(B.B200Error) as e:
+                call()
+            assert e.value.code == -1 and "peer mapping" in str(e.value)
+    for partials in ([B.ptr(0, src), end + 4096], [base - 4096, base]):
+        with pytest.raises(B.B200Error) as e:
+            B.span_combine("sum", "float32", 2, 0, partials, dst, 0, team=team)
+        assert e.value.code == -1 and "peer mapping" in str(e.value)
