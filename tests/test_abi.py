@@ -39,6 +39,17 @@ def test_calls_before_init_fail_with_state_error():
     assert L.b200shm_fcollect(0, 1, 4, 0, 0, 64, None) == -5
     assert L.b200shm_barrier(2, 0, 1, 4, None) == -5
     assert L.b200shm_ptr(0, 0) is None
+    # the span calls check the team (and so the engine) before any address
+    addrs = (ctypes.c_uint64 * 2)(1 << 40, 1 << 41)
+    assert L.b200shm_span_fcollect(2, 0, addrs, 0, 1, 4, 0, 0, 64, None) == -5
+    assert L.b200shm_span_alltoall(2, 0, addrs, 0, 1, 4, 0, 0, 64, None) == -5
+    assert L.b200shm_span_combine(5, 8, 2, 0, addrs, 0, 1, 4, 0, 16, None) == -5
+    assert L.b200shm_span_amo(0, 3, 2, addrs, 0, 1, 4, 0, None, None, None, None, None,
+                              None) == -5
+    assert b"not initialised" in L.b200shm_last_error()
+    # a bad rank count or rank is refused first, engine or not
+    assert L.b200shm_span_fcollect(3, 0, addrs, 0, 1, 4, 0, 0, 64, None) == -1
+    assert L.b200shm_span_alltoall(2, 2, addrs, 0, 1, 4, 0, 0, 64, None) == -1
 
 
 def test_shmem_surface_exports_every_declared_function():
